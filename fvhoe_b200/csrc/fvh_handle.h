@@ -1,0 +1,70 @@
+// Solver handle shared by the C ABI (fvh_api.cu) and the per-precision stage
+// runners (fvh_stage_f64.cu, fvh_stage_f32.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "fvh.h"
+#include "fvh_kernels.cuh"
+#include "fvh_profile.h"
+
+struct fvh_handle {
+  fvh_config cfg;
+  int nv = 5;
+  int n[3] = {1, 1, 1};
+  int p[3] = {0, 0, 0};
+  int r[3] = {0, 0, 0};           // stencil radius ceil(p/2) per axis
+  bool active[3] = {false, false, false};
+  int ndim = 0;
+  int gw = 0;                     // ghost width of the high-order flux pass
+  int gW = 0;                     // ghost width of the primitive array W
+  double cfl_h = 0.0;             // CFL * min(h)
+  double neg_inv_h[3] = {0, 0, 0};
+  fvh::Grid grid{};
+  size_t elem = 8;                // bytes of the compute type
+
+  // device memory owned by the handle
+  void* bufA = nullptr;           // sweep scratch (ping)
+  void* bufB = nullptr;           // sweep scratch (pong)
+  size_t buf_elems = 0;
+  void* W = nullptr;              // FV primitives of the stage input, gW ghosts
+  void* Ws = nullptr;             // FV primitives of the candidate, 3 ghosts
+  double* Us = nullptr;           // candidate state
+  void* F[3] = {nullptr, nullptr, nullptr};      // face fluxes per axis
+  float* theta[3] = {nullptr, nullptr, nullptr}; // convex face weights per axis
+  float* conv = nullptr;                          // convex work arrays (3 padded boxes)
+  uint8_t* trouble = nullptr;
+  double* logs[3] = {nullptr, nullptr, nullptr};  // running trouble / NAD / PAD sums
+  double* acc = nullptr;          // running k-sum of ssprk3 / rk4
+  double* S[2] = {nullptr, nullptr};              // stage inputs
+  fvh::Scalars* sc = nullptr;
+  size_t scratch_bytes = 0;
+
+  int log_mode_next = 1;          // log mode of the next stage
+  fvh::Profiler* prof = nullptr;  // per-launch timing, when enabled
+  fvh::KernelTotals prof_totals{};
+  std::string err;
+};
+
+namespace fvh {
+
+struct StageCall {
+  const double* stage_in;  // input state of this stage
+  StageSpec spec;          // Runge-Kutta epilogue
+  int first_stage;         // fixes the step's dt
+  int has_target;
+  double t;
+  double target;
+  int log_mode;            // 0 none, 1 overwrite, 2 add
+};
+
+// Runs one stage on the stream; returns an FVH_ status.
+int run_stage_f64(fvh_handle* h, const StageCall& c, cudaStream_t s);
+int run_stage_f32(fvh_handle* h, const StageCall& c, cudaStream_t s);
+
+// FV primitives of u over the interior (snapshot conversion).
+int primitives_f64(fvh_handle* h, const double* u, double* w, int fv_average, cudaStream_t s);
+
+}  // namespace fvh

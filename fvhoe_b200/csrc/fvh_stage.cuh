@@ -1,0 +1,508 @@
+// Host orchestration of one stage of the per-stage update, templated on the
+// compute type. Included once by fvh_stage_f64.cu (built with -fmad=false,
+// bit-exact with the reference) and once by fvh_stage_f32.cu.
+//
+// Pass sequence of one stage (fvhoe/solver.py:429-454):
+//   1. W  = FV primitives of the stage input with gW ghosts, plus the CFL
+//           maximum over the gw-ghost box and the per-variable extrema over
+//           the 3-ghost box                  (solver.py:491-517, 686)
+//   2. dt = CFL h / max, or fixed_dt; stage 0 also clamps to the target
+//   3. per active axis d: centre sweeps along the other axes, face states +
+//      Riemann solve along d, transverse sweeps          (solver.py:519-651)
+//   4. a-posteriori limiting (solver.py:653-732): candidate u*, W* of u*,
+//      detection, convex weights, MUSCL fallback + blend at troubled faces
+//   5. flux divergence + Runge-Kutta stage combination   (solver.py:734-751)
+#pragma once
+
+#include <algorithm>
+#include <cstdio>
+#include <string>
+
+#include "fvh_handle.h"
+#include "fvh_profile.h"
+
+namespace fvh {
+
+// ---------------------------------------------------------------------------
+// stencil rules (fvhoe/stencils.py:25-255), stored as exact rationals; the
+// float64 weight is the correctly rounded quotient, as the reference's `a / b`
+// literals evaluate. Centre and transverse rules of odd p equal the rule of
+// p - 1 (their extra end taps are zero), so only even degrees are stored.
+// ---------------------------------------------------------------------------
+struct HostRule {
+  int K = 1;
+  int off = 0;
+  double w[9] = {1, 0, 0, 0, 0, 0, 0, 0, 0};
+};
+
+inline HostRule make_rule(long long den, const long long* num, int K) {
+  HostRule r;
+  r.K = K;
+  r.off = -(K - 1) / 2;
+  for (int k = 0; k < K; ++k) r.w[k] = (double)num[k] / (double)den;
+  return r;
+}
+
+inline HostRule left_face_rule(int p) {
+  static const long long den[9] = {1, 4, 6, 24, 60, 120, 420, 1680, 2520};
+  static const long long num[9][9] = {
+      {1},
+      {1, 4, -1},
+      {2, 5, -1},
+      {-1, 10, 20, -6, 1},
+      {-3, 27, 47, -13, 2},
+      {1, -10, 59, 94, -31, 8, -1},
+      {4, -38, 214, 319, -101, 25, -3},
+      {-3, 34, -194, 898, 1276, -446, 142, -30, 3},
+      {-5, 55, -305, 1375, 1879, -641, 199, -41, 4},
+  };
+  const int K = 2 * ((p + 1) / 2) + 1;
+  return make_rule(den[p], num[p], K);
+}
+
+inline HostRule right_face_rule(int p) {
+  HostRule l = left_face_rule(p);
+  HostRule r = l;
+  for (int k = 0; k < l.K; ++k) r.w[k] = l.w[l.K - 1 - k];
+  return r;
+}
+
+inline HostRule centre_rule(int p) {
+  static const long long den[5] = {1, 24, 1920, 107520, 10321920};
+  static const long long num[5][9] = {
+      {1},
+      {-1, 26, -1},
+      {9, -116, 2134, -116, 9},
+      {-75, 954, -7621, 121004, -7621, 954, -75},
+      {1225, -17000, 125884, -800216, 11702134, -800216, 125884, -17000, 1225},
+  };
+  const int e = p / 2;
+  return make_rule(den[e], num[e], 2 * e + 1);
+}
+
+inline HostRule transverse_rule(int p) {
+  static const long long den[5] = {1, 24, 5760, 967680, 464486400};
+  static const long long num[5][9] = {
+      {1},
+      {1, 22, 1},
+      {-17, 308, 5178, 308, -17},
+      {367, -5058, 57249, 862564, 57249, -5058, 367},
+      {-27859, 399032, -3207892, 29039624, 412080590, 29039624, -3207892, 399032, -27859},
+  };
+  const int e = p / 2;
+  return make_rule(den[e], num[e], 2 * e + 1);
+}
+
+template <typename Tc, int K>
+inline Rule<Tc, K> device_rule(const HostRule& hr) {
+  Rule<Tc, K> r;
+  for (int k = 0; k < K; ++k) r.w[k] = (Tc)hr.w[k];
+  r.off = hr.off;
+  return r;
+}
+
+inline unsigned blocks_for(int64_t n, int threads = 256) {
+  int64_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > (1 << 22)) b = 1 << 22;
+  return (unsigned)b;
+}
+
+// bytes of nv variables of `elem` bytes over r, with r grown by `grow` cells along `axis`
+inline double region_bytes(const Region& r, int nv, size_t elem, int axis = -1, int grow = 0) {
+  double pts = 1.0;
+  for (int a = 0; a < 3; ++a) pts *= (double)(r.n[a] + (a == axis ? grow : 0));
+  return pts * nv * (double)elem;
+}
+
+inline Region interior_region(const fvh_handle* h) {
+  Region r;
+  for (int a = 0; a < 3; ++a) {
+    r.lo[a] = 0;
+    r.n[a] = h->n[a];
+  }
+  return r;
+}
+
+// Box [-g, n+g) on the active axes, interior extent elsewhere.
+inline Region padded_region(const fvh_handle* h, int g) {
+  Region r;
+  for (int a = 0; a < 3; ++a) {
+    const int ga = h->active[a] ? g : 0;
+    r.lo[a] = -ga;
+    r.n[a] = h->n[a] + 2 * ga;
+  }
+  return r;
+}
+
+inline Region face_region(const fvh_handle* h, int d) {
+  Region r = interior_region(h);
+  r.n[d] += 1;
+  return r;
+}
+
+inline int set_cuda_error(fvh_handle* h, const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return FVH_OK;
+  h->err = std::string(what) + ": " + cudaGetErrorString(e);
+  return FVH_ERR_CUDA;
+}
+
+template <typename Tc>
+inline Phys<Tc> make_phys(const fvh_handle* h) {
+  Phys<Tc> ph;
+  ph.gamma = (Tc)h->cfg.gamma;
+  ph.gm1 = (Tc)(h->cfg.gamma - 1.0);
+  ph.csq_floor = (Tc)h->cfg.csq_floor;
+  ph.nv = h->nv;
+  ph.riemann = h->cfg.riemann;
+  ph.pad_ = 0;
+  return ph;
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers: dispatch the tap count K to a compile-time constant
+// ---------------------------------------------------------------------------
+template <typename Tc, int NV, int K>
+void launch_centre_k(bool from_state, bool to_prims, const void* in, Region rin, Tc* out, Region rout, int axis,
+                     const HostRule& hr, const Grid& g, const Phys<Tc>& ph, cudaStream_t s) {
+  const Rule<Tc, K> rule = device_rule<Tc, K>(hr);
+  const unsigned nb = blocks_for(region_points(rout));
+  LaunchScope scope(KK_CENTRE,
+                    region_bytes(rout, ph.nv, from_state ? sizeof(double) : sizeof(Tc), axis, K - 1) +
+                        region_bytes(rout, ph.nv, sizeof(Tc)),
+                    s);
+  if (from_state) {
+    if (to_prims)
+      k_centre_sweep<Tc, double, NV, K, true, true>
+          <<<nb, 256, 0, s>>>((const double*)in, rin, out, rout, axis, rule, g, ph);
+    else
+      k_centre_sweep<Tc, double, NV, K, true, false>
+          <<<nb, 256, 0, s>>>((const double*)in, rin, out, rout, axis, rule, g, ph);
+  } else {
+    if (to_prims)
+      k_centre_sweep<Tc, Tc, NV, K, false, true><<<nb, 256, 0, s>>>((const Tc*)in, rin, out, rout, axis, rule, g, ph);
+    else
+      k_centre_sweep<Tc, Tc, NV, K, false, false><<<nb, 256, 0, s>>>((const Tc*)in, rin, out, rout, axis, rule, g, ph);
+  }
+}
+
+template <typename Tc, int NV>
+void launch_centre(bool from_state, bool to_prims, const void* in, Region rin, Tc* out, Region rout, int axis,
+                   const HostRule& hr, const Grid& g, const Phys<Tc>& ph, cudaStream_t s) {
+  switch (hr.K) {
+    case 1: launch_centre_k<Tc, NV, 1>(from_state, to_prims, in, rin, out, rout, axis, hr, g, ph, s); break;
+    case 3: launch_centre_k<Tc, NV, 3>(from_state, to_prims, in, rin, out, rout, axis, hr, g, ph, s); break;
+    case 5: launch_centre_k<Tc, NV, 5>(from_state, to_prims, in, rin, out, rout, axis, hr, g, ph, s); break;
+    case 7: launch_centre_k<Tc, NV, 7>(from_state, to_prims, in, rin, out, rout, axis, hr, g, ph, s); break;
+    case 9: launch_centre_k<Tc, NV, 9>(from_state, to_prims, in, rin, out, rout, axis, hr, g, ph, s); break;
+  }
+}
+
+template <typename Tc, int NV, int K>
+void launch_transverse_k(bool reduce, const Tc* in, Region rin, Tc* out, Region rout, int axis, const HostRule& hr,
+                         const Phys<Tc>& ph, const ReduceSpec& rs, Scalars* sc, cudaStream_t s) {
+  const Rule<Tc, K> rule = device_rule<Tc, K>(hr);
+  const unsigned nb = blocks_for(region_points(rout));
+  LaunchScope scope(KK_TRANSVERSE,
+                    region_bytes(rout, ph.nv, sizeof(Tc), axis, K - 1) + region_bytes(rout, ph.nv, sizeof(Tc)), s);
+  if (reduce)
+    k_transverse_sweep<Tc, NV, K, true><<<nb, 256, 0, s>>>(in, rin, out, rout, axis, rule, ph, rs, sc);
+  else
+    k_transverse_sweep<Tc, NV, K, false><<<nb, 256, 0, s>>>(in, rin, out, rout, axis, rule, ph, rs, sc);
+}
+
+template <typename Tc, int NV>
+void launch_transverse(bool reduce, const Tc* in, Region rin, Tc* out, Region rout, int axis, const HostRule& hr,
+                       const Phys<Tc>& ph, const ReduceSpec& rs, Scalars* sc, cudaStream_t s) {
+  switch (hr.K) {
+    case 1: launch_transverse_k<Tc, NV, 1>(reduce, in, rin, out, rout, axis, hr, ph, rs, sc, s); break;
+    case 3: launch_transverse_k<Tc, NV, 3>(reduce, in, rin, out, rout, axis, hr, ph, rs, sc, s); break;
+    case 5: launch_transverse_k<Tc, NV, 5>(reduce, in, rin, out, rout, axis, hr, ph, rs, sc, s); break;
+    case 7: launch_transverse_k<Tc, NV, 7>(reduce, in, rin, out, rout, axis, hr, ph, rs, sc, s); break;
+    case 9: launch_transverse_k<Tc, NV, 9>(reduce, in, rin, out, rout, axis, hr, ph, rs, sc, s); break;
+  }
+}
+
+template <typename Tc, int NV, int K>
+void launch_face_k(const Tc* in, Region rin, Tc* out, Region rout, int d, const HostRule& l, const HostRule& r,
+                   const Phys<Tc>& ph, cudaStream_t s) {
+  LaunchScope scope(KK_FACE, region_bytes(rout, ph.nv, sizeof(Tc), d, K) + region_bytes(rout, ph.nv, sizeof(Tc)), s);
+  k_face_riemann<Tc, NV, K><<<blocks_for(region_points(rout)), 256, 0, s>>>(
+      in, rin, out, rout, d, device_rule<Tc, K>(l), device_rule<Tc, K>(r), ph);
+}
+
+template <typename Tc, int NV>
+void launch_face(const Tc* in, Region rin, Tc* out, Region rout, int d, const HostRule& l, const HostRule& r,
+                 const Phys<Tc>& ph, cudaStream_t s) {
+  switch (l.K) {
+    case 1: launch_face_k<Tc, NV, 1>(in, rin, out, rout, d, l, r, ph, s); break;
+    case 3: launch_face_k<Tc, NV, 3>(in, rin, out, rout, d, l, r, ph, s); break;
+    case 5: launch_face_k<Tc, NV, 5>(in, rin, out, rout, d, l, r, ph, s); break;
+    case 7: launch_face_k<Tc, NV, 7>(in, rin, out, rout, d, l, r, ph, s); break;
+    case 9: launch_face_k<Tc, NV, 9>(in, rin, out, rout, d, l, r, ph, s); break;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FV primitives with g ghost cells (fvhoe/solver.py:753-792):
+// ghost-fill u with g + 2r cells through the index maps, centre sweeps along
+// x, y, z (the last converts to primitives), transverse sweeps along x, y, z
+// (the last writes dst and performs the requested reductions).
+// With fv_average = false only the centre sweeps run, with g + r ghosts.
+// ---------------------------------------------------------------------------
+template <typename Tc, int NV>
+int primitive_pass(fvh_handle* h, const double* state, int g, Tc* dst, const ReduceSpec& rs, bool reduce,
+                   bool fv_average, cudaStream_t s) {
+  const Phys<Tc> ph = make_phys<Tc>(h);
+  int axes[3], na = 0;
+  for (int a = 0; a < 3; ++a)
+    if (h->active[a]) axes[na++] = a;
+  Region cur;
+  const int grow = fv_average ? 2 : 1;
+  for (int a = 0; a < 3; ++a) {
+    const int ga = h->active[a] ? g + grow * h->r[a] : 0;
+    cur.lo[a] = -ga;
+    cur.n[a] = h->n[a] + 2 * ga;
+  }
+  Tc* bufs[2] = {(Tc*)h->bufA, (Tc*)h->bufB};
+  int which = 0;
+  const void* src = state;
+  Region rsrc = cur;
+  for (int q = 0; q < na; ++q) {
+    const int a = axes[q];
+    Region out = cur;
+    const int ga = fv_average ? g + h->r[a] : g;
+    out.lo[a] = -ga;
+    out.n[a] = h->n[a] + 2 * ga;
+    const bool last = (q == na - 1);
+    Tc* o = (last && !fv_average) ? dst : bufs[which];
+    launch_centre<Tc, NV>(q == 0, last, src, rsrc, o, out, a, centre_rule(h->p[a]), h->grid, ph, s);
+    src = o;
+    rsrc = out;
+    cur = out;
+    which ^= 1;
+  }
+  if (fv_average) {
+    for (int q = 0; q < na; ++q) {
+      const int a = axes[q];
+      Region out = cur;
+      out.lo[a] = -g;
+      out.n[a] = h->n[a] + 2 * g;
+      const bool last = (q == na - 1);
+      Tc* o = last ? dst : bufs[which];
+      launch_transverse<Tc, NV>(last && reduce, (const Tc*)src, rsrc, o, out, a, transverse_rule(h->p[a]), ph, rs,
+                                h->sc, s);
+      src = o;
+      rsrc = out;
+      cur = out;
+      which ^= 1;
+    }
+  }
+  return set_cuda_error(h, "primitive pass");
+}
+
+// ---------------------------------------------------------------------------
+// High-order face fluxes along d from W (fvhoe/solver.py:519-651).
+// ---------------------------------------------------------------------------
+template <typename Tc, int NV>
+int flux_pass(fvh_handle* h, const Tc* W, Region rW, int d, Tc* Fd, cudaStream_t s) {
+  const Phys<Tc> ph = make_phys<Tc>(h);
+  Tc* bufs[2] = {(Tc*)h->bufA, (Tc*)h->bufB};
+  int which = 0;
+  // restrict the source box to what the faces of the interior need
+  Region cur = rW;
+  cur.lo[d] = -(h->r[d] + 1);
+  cur.n[d] = h->n[d] + 2 * (h->r[d] + 1);
+  for (int t = 0; t < 3; ++t) {
+    if (t == d || !h->active[t]) continue;
+    cur.lo[t] = -2 * h->r[t];
+    cur.n[t] = h->n[t] + 4 * h->r[t];
+  }
+  const Tc* src = W;
+  Region rsrc = rW;
+  // centre sweeps along (d+2)%3 then (d+1)%3 (fvhoe/solver.py:523-568)
+  const int order[2] = {(d + 2) % 3, (d + 1) % 3};
+  for (int q = 0; q < 2; ++q) {
+    const int t = order[q];
+    if (!h->active[t]) continue;
+    Region out = cur;
+    out.lo[t] = -h->r[t];
+    out.n[t] = h->n[t] + 2 * h->r[t];
+    Tc* o = bufs[which];
+    launch_centre<Tc, NV>(false, false, src, rsrc, o, out, t, centre_rule(h->p[t]), h->grid, ph, s);
+    src = o;
+    rsrc = out;
+    cur = out;
+    which ^= 1;
+  }
+  // face states along d and the Riemann solve
+  int others[2], no = 0;
+  for (int t = 0; t < 3; ++t)
+    if (t != d && h->active[t]) others[no++] = t;
+  Region rf = cur;
+  rf.lo[d] = 0;
+  rf.n[d] = h->n[d] + 1;
+  for (int t = 0; t < 3; ++t)
+    if (t != d && !h->active[t]) {
+      rf.lo[t] = 0;
+      rf.n[t] = 1;
+    }
+  Tc* o = (no == 0) ? Fd : bufs[which];
+  launch_face<Tc, NV>(src, rsrc, o, rf, d, left_face_rule(h->p[d]), right_face_rule(h->p[d]), ph, s);
+  src = o;
+  rsrc = rf;
+  which ^= 1;
+  // transverse sweeps along the other axes in ascending order (solver.py:629-648)
+  Region c2 = rf;
+  for (int q = 0; q < no; ++q) {
+    const int t = others[q];
+    Region out = c2;
+    out.lo[t] = 0;
+    out.n[t] = h->n[t];
+    Tc* dst = (q == no - 1) ? Fd : bufs[which];
+    ReduceSpec none{};
+    launch_transverse<Tc, NV>(false, src, rsrc, dst, out, t, transverse_rule(h->p[t]), ph, none, h->sc, s);
+    src = dst;
+    rsrc = out;
+    c2 = out;
+    which ^= 1;
+  }
+  return set_cuda_error(h, "flux pass");
+}
+
+// ---------------------------------------------------------------------------
+// Convex face weights (fvhoe/slope_limiting.py:281-363, 387-442): applied as
+// the reference's sequence of shifted maxima on a trouble array padded by 2
+// zero cells on the active axes. (The reference's periodic wrap of this
+// padding writes an empty slice unless all three axes are active, so the
+// padding stays zero in 1D and 2D.)
+// ---------------------------------------------------------------------------
+__global__ void k_convex_init(const uint8_t* __restrict__ trouble, Region rint, Region rpad, float* __restrict__ th);
+__global__ void k_convex_step(const float* __restrict__ src, const float* __restrict__ prev, float* __restrict__ out,
+                              Region rpad, int s0, int s1, int s2, float coef, int src_is_theta);
+__global__ void k_convex_faces(const float* __restrict__ th, Region rpad, float* __restrict__ theta, Region rflux,
+                               int d);
+
+int convex_weights(fvh_handle* h, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// one stage
+// ---------------------------------------------------------------------------
+template <typename Tc, int NV>
+int run_stage_t(fvh_handle* h, const StageCall& c, cudaStream_t s) {
+  const Phys<Tc> ph = make_phys<Tc>(h);
+  const fvh_config& cfg = h->cfg;
+  const bool apost = cfg.a_posteriori != 0;
+  int st;
+  {
+    LaunchScope scope(KK_SMALL, 0.0, s);
+    k_reset_scalars<<<1, 32, 0, s>>>(h->sc, c.first_stage);
+  }
+  // 1. FV primitives of the stage input
+  ReduceSpec rs{};
+  rs.cfl = cfg.use_fixed_dt ? 0 : 1;
+  rs.cfl_box = padded_region(h, h->gw);
+  rs.extrema = (apost && cfg.nad_global) ? 1 : 0;
+  rs.ext_box = padded_region(h, 3);
+  rs.ndim = (double)h->ndim;
+  const Region rW = padded_region(h, h->gW);
+  if ((st = primitive_pass<Tc, NV>(h, c.stage_in, h->gW, (Tc*)h->W, rs, true, true, s))) return st;
+  // 2. dt
+  {
+    LaunchScope scope(KK_SMALL, 0.0, s);
+    k_finalize_dt<<<1, 1, 0, s>>>(h->sc, h->cfl_h, cfg.use_fixed_dt, cfg.fixed_dt, c.first_stage, c.has_target,
+                                  c.t, c.target);
+  }
+  // 3. high-order fluxes
+  FluxSet fs{};
+  for (int d = 0; d < 3; ++d) {
+    if (!h->active[d]) continue;
+    if ((st = flux_pass<Tc, NV>(h, (const Tc*)h->W, rW, d, (Tc*)h->F[d], s))) return st;
+    fs.f[d] = h->F[d];
+    fs.r[d] = face_region(h, d);
+    fs.neg_inv_h[d] = h->neg_inv_h[d];
+  }
+  const Region rint = interior_region(h);
+  double flux_bytes = 0.0;
+  for (int d = 0; d < 3; ++d)
+    if (h->active[d]) flux_bytes += region_bytes(face_region(h, d), h->nv, sizeof(Tc));
+  const double state_bytes = region_bytes(rint, h->nv, sizeof(double));
+  // 4. a-posteriori limiting
+  if (apost) {
+    {
+      LaunchScope scope(KK_CANDIDATE, 2 * state_bytes + flux_bytes, s);
+      k_candidate<Tc, NV><<<blocks_for(region_points(rint)), 256, 0, s>>>(c.stage_in, rint, fs, h->Us, ph, h->sc);
+    }
+    if ((st = set_cuda_error(h, "candidate"))) return st;
+    ReduceSpec none{};
+    if ((st = primitive_pass<Tc, NV>(h, h->Us, 3, (Tc*)h->Ws, none, false, true, s))) return st;
+    DetectSpec ds{};
+    ds.nad_global = cfg.nad_global;
+    ds.nad_relative = cfg.nad_relative;
+    ds.nad_eps = cfg.nad_eps;
+    ds.nad_var_mask = cfg.nad_var_mask;
+    ds.sed = cfg.sed;
+    ds.sed_eps = cfg.sed_eps;
+    ds.pad_var = cfg.pad_var;
+    ds.pad_lo = cfg.pad_lo;
+    ds.pad_hi = cfg.pad_hi;
+    ds.force_trouble = cfg.force_trouble;
+    for (int a = 0; a < 3; ++a) ds.active[a] = h->active[a] ? 1 : 0;
+    ds.log_mode = cfg.log_troubles ? c.log_mode : 0;
+    {
+      const double log_bytes = ds.log_mode ? 3.0 * (ds.log_mode == 2 ? 2 : 1) * region_bytes(rint, 1, 8) : 0.0;
+      LaunchScope scope(KK_DETECT,
+                        region_bytes(padded_region(h, 1), 5, sizeof(Tc)) + region_bytes(padded_region(h, 3), 5,
+                                                                                         sizeof(Tc)) +
+                            region_bytes(rint, 1, 1) + log_bytes,
+                        s);
+      k_detect<Tc><<<blocks_for(region_points(rint)), 256, 0, s>>>((const Tc*)h->W, rW, (const Tc*)h->Ws,
+                                                                   padded_region(h, 3), rint, ds, h->sc, h->trouble,
+                                                                   h->logs[0], h->logs[1], h->logs[2]);
+    }
+    if ((st = set_cuda_error(h, "detect"))) return st;
+    if (cfg.convex) {
+      if ((st = convex_weights(h, s))) return st;
+    }
+    for (int d = 0; d < 3; ++d) {
+      if (!h->active[d]) continue;
+      FallbackSpec fb{};
+      fb.d = d;
+      fb.muscl = h->p[d] > 0 ? 1 : 0;
+      fb.limiter = cfg.slope_limiter;
+      fb.rflux = face_region(h, d);
+      fb.rint = rint;
+      {
+        LaunchScope scope(KK_FALLBACK,
+                          region_bytes(rint, 1, 1) + state_bytes + 2 * region_bytes(fb.rflux, h->nv, sizeof(Tc)), s);
+        k_fallback<Tc, NV><<<blocks_for(region_points(fb.rflux)), 256, 0, s>>>(
+            c.stage_in, h->grid, (Tc*)h->F[d], h->trouble, cfg.convex ? h->theta[d] : nullptr, fb, ph);
+      }
+      if ((st = set_cuda_error(h, "fallback"))) return st;
+    }
+  }
+  // 5. divergence + Runge-Kutta combination
+  {
+    // state arrays read and written by the Runge-Kutta combination of this stage
+    int arrays = 1;
+    switch (c.spec.integrator) {
+      case INT_EULER: arrays = 2; break;
+      case INT_SSPRK2: arrays = c.spec.stage == 0 ? 2 : 3; break;
+      case INT_SSPRK3: arrays = c.spec.stage == 1 ? 4 : 3; break;
+      case INT_RK4: arrays = c.spec.stage == 0 ? 3 : (c.spec.stage == 3 ? 3 : 4); break;
+      default: arrays = 1; break;
+    }
+    LaunchScope scope(KK_FINAL, flux_bytes + arrays * state_bytes, s);
+    k_final<Tc, NV><<<blocks_for(region_points(rint)), 256, 0, s>>>(rint, fs, ph, c.spec, h->sc);
+  }
+  return set_cuda_error(h, "final");
+}
+
+template <typename Tc>
+int run_stage_any(fvh_handle* h, const StageCall& c, cudaStream_t s) {
+  if (h->nv == 5) return run_stage_t<Tc, 5>(h, c, s);
+  return run_stage_t<Tc, 0>(h, c, s);
+}
+
+}  // namespace fvh

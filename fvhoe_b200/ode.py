@@ -1,0 +1,143 @@
+"""Time-integration driver (host side).
+
+Same interface as fvhoe/ode.py:25-298 (`ODE`): integrate(T, n, exact,
+downbeats, log_every_step, snapshot_dir, overwrite) and the steppers euler,
+ssprk2, ssprk3 and rk4, each of which records its name and integrates. The
+loop, the downbeat bookkeeping and the snapshot cadence are the reference's;
+one step is a single call into the CUDA library (`_device_step`), which runs
+all stages of the chosen integrator on the device and returns the step's dt
+(shortened to the next downbeat when `exact`, fvhoe/ode.py:11-22).
+"""
+
+import os
+from abc import ABC, abstractmethod
+from typing import Any, Optional
+
+import numpy as np
+
+from .timer import Timer
+
+
+def _hit_target(t: float, dt: float, target: float = None) -> float:
+    """dt shortened so that t + dt does not pass target (fvhoe/ode.py:11-22)."""
+    if target is not None and target - t < dt:
+        return target - t
+    return dt
+
+
+class ODE(ABC):
+    def _ode_init(self, progress_bar: bool = True):
+        self.t = 0.0
+        self.timestamps = [0.0]
+        self.step_count = 0
+        self.timer = Timer(cats=["TOTAL", "SNAPSHOTS"])
+        self.snapshots = []
+        self.snapshot_times = []
+        self.print_progress_bar = bool(progress_bar)
+        self.integrator = None
+
+    # -- stepping -----------------------------------------------------------
+    @abstractmethod
+    def _device_step(self, integrator: str, target_time: Optional[float]) -> float:
+        """Advance am("u") by one step in place and return dt."""
+
+    @abstractmethod
+    def f(self, t: float, u) -> tuple:
+        """(dt, dudt) of one right-hand-side evaluation."""
+
+    def take_step(self, target_time: float = None):
+        dt = self._device_step(self.integrator, target_time)
+        self.t += dt
+        self.timestamps.append(self.t)
+        self.step_count += 1
+        self.step_helper_function()
+
+    def step_helper_function(self):
+        pass
+
+    def snapshot(self):
+        self.snapshots.append(None)
+        self.snapshot_times.append(self.t)
+
+    def read_snapshots(self) -> bool:
+        return False
+
+    def write_snapshots(self, overwrite: bool = False):
+        pass
+
+    # -- driver (fvhoe/ode.py:94-174) ------------------------------------------
+    def integrate(self, T: float = None, n: int = None, exact: bool = True, downbeats: Any = None,
+                  log_every_step: bool = False, snapshot_dir: str = None, overwrite: bool = False) -> None:
+        if T is None:
+            self.timer.start("SNAPSHOTS")
+            self.snapshot()
+            self.timer.stop("SNAPSHOTS")
+            self.timer.start("TOTAL")
+            for _ in self._progress(range(n)):
+                self.take_step()
+            self.timer.stop("TOTAL")
+            self.timer.start("SNAPSHOTS")
+            self.snapshot()
+            self.timer.stop("SNAPSHOTS")
+            return
+        save = snapshot_dir is not None
+        if save:
+            self.snapshot_dir = os.path.normpath(snapshot_dir)
+            if not overwrite and self.read_snapshots():
+                return
+        bar = self._bar(T)
+        if downbeats is None:
+            downbeats = []
+        elif isinstance(downbeats, np.ndarray):
+            downbeats = downbeats.tolist()
+        downbeats = sorted(set([0] + list(downbeats) + [T]))[1:]
+        target_time = downbeats.pop(0) if exact else None
+        self.snapshot()
+        self.timer.start("TOTAL")
+        while self.t < T:
+            self.take_step(target_time=target_time)
+            if bar is not None:
+                bar.n = self.t
+                bar.refresh()
+            if self.t == target_time or self.t >= T or log_every_step:
+                self.timer.start("SNAPSHOTS")
+                self.snapshot()
+                self.timer.stop("SNAPSHOTS")
+                if downbeats and self.t == target_time:
+                    target_time = downbeats.pop(0)
+        self.timer.stop("TOTAL")
+        if bar is not None:
+            bar.close()
+        if save:
+            self.write_snapshots(overwrite)
+
+    def _progress(self, it):
+        if not self.print_progress_bar:
+            return it
+        from tqdm import tqdm
+
+        return tqdm(it)
+
+    def _bar(self, T):
+        if not self.print_progress_bar:
+            return None
+        from tqdm import tqdm
+
+        return tqdm(total=T, bar_format="{l_bar}{bar}| {n_fmt}/{total_fmt} [{elapsed}]")
+
+    # -- steppers (fvhoe/ode.py:245-298) ------------------------------------------
+    def euler(self, *args, **kwargs) -> None:
+        self.integrator = "euler"
+        self.integrate(*args, **kwargs)
+
+    def ssprk2(self, *args, **kwargs) -> None:
+        self.integrator = "ssprk2"
+        self.integrate(*args, **kwargs)
+
+    def ssprk3(self, *args, **kwargs) -> None:
+        self.integrator = "ssprk3"
+        self.integrate(*args, **kwargs)
+
+    def rk4(self, *args, **kwargs) -> None:
+        self.integrator = "rk4"
+        self.integrate(*args, **kwargs)

@@ -1,0 +1,453 @@
+"""EulerSolver with the "cuda" array backend.
+
+The constructor takes the arguments of fvhoe/solver.py:42-84 (plus
+`backend`, `precision` and `log_troubles`), builds the mesh and the initial
+condition on the host exactly as the reference does (fvhoe/solver.py:220-312),
+moves the state to the GPU once, and from then on every right-hand-side
+evaluation and every time step runs in the CUDA library libfvh.so through its
+C ABI (include/fvh.h). Snapshots, trouble logs, timing categories and the
+snapshot files keep the reference's formats (fvhoe/solver.py:794-953).
+
+There is no CPU path: constructing the solver without a CUDA device, or
+without the built library, raises.
+"""
+
+import ctypes
+import inspect
+import json
+import os
+import pickle
+import shutil
+from typing import Callable, Dict, Iterable, Tuple
+
+import numpy as np
+
+from .array_management import ArrayManager
+from .boundary_conditions import BoundaryCondition
+from .fv import fv_average, fv_uniform_meshgen
+from .hydro import HydroState, compute_conservatives
+from .initial_conditions import InitialCondition, Square
+from .ode import ODE
+
+_VAR_INDEX = {"rho": 0, "vx": 1, "mx": 1, "vy": 2, "my": 2, "vz": 3, "mz": 3, "P": 4, "E": 4}
+_STAGES = {"euler": 1, "ssprk2": 2, "ssprk3": 3, "rk4": 4}
+
+
+class EulerSolver(ODE):
+    def __init__(
+        self,
+        w0: InitialCondition = None,
+        w0_passives: Dict[str, Callable] = None,
+        nx: int = 1,
+        ny: int = 1,
+        nz: int = 1,
+        px: int = 0,
+        py: int = 0,
+        pz: int = 0,
+        x: Tuple[float, float] = (0, 1),
+        y: Tuple[float, float] = (0, 1),
+        z: Tuple[float, float] = (0, 1),
+        CFL: float = 0.8,
+        fixed_dt: float = None,
+        gamma: float = 5 / 3,
+        bc: BoundaryCondition = None,
+        riemann_solver: str = "hllc",
+        conservative_ic: bool = False,
+        fv_ic: bool = False,
+        fixed_primitive_variables: Iterable = None,
+        a_posteriori_slope_limiting: bool = False,
+        slope_limiter: str = "minmod",
+        force_trouble: bool = False,
+        NAD: float = 1e-2,
+        NAD_mode: str = "global",
+        NAD_range: str = "relative",
+        NAD_vars: tuple = None,
+        PAD: dict = None,
+        SED: bool = True,
+        SED_tolerance: float = 1e-10,
+        convex: bool = False,
+        density_floor: float = None,
+        pressure_floor: float = None,
+        csq_floor: float = 1e-10,
+        progress_bar: bool = True,
+        snapshots_as_fv_averages: bool = True,
+        snapshot_helper_function: callable = None,
+        slab_buffer_size: int = 30,
+        cupy: bool = False,
+        backend: str = None,
+        precision: str = "fp64",
+        log_troubles: bool = True,
+    ):
+        if backend is None:
+            backend = os.environ.get("FVHOE_BACKEND", "cuda")
+        if backend != "cuda":
+            raise ValueError("this EulerSolver runs on the 'cuda' backend only")
+        if precision not in ("fp64", "fp32"):
+            raise ValueError("precision must be 'fp64' or 'fp32'")
+        from . import _capi  # raises when libfvh.so is missing
+
+        self._capi = _capi
+        self.backend = backend
+        self.precision = precision
+        self.csq_floor = csq_floor
+        self.density_floor = density_floor
+        self.gamma = gamma
+        self.pressure_floor = pressure_floor
+        self.riemann_solver_name = riemann_solver
+        self.snapshot_helper_function = snapshot_helper_function
+        self.snapshots_as_fv_averages = snapshots_as_fv_averages
+        self.fixed_primitive_variables = fixed_primitive_variables
+        self.slab_buffer_size = slab_buffer_size
+        if riemann_solver not in _capi.RIEMANN:
+            raise TypeError(f"Invalid Riemann solver {riemann_solver}")
+        self._init_mesh(x, y, z, nx, ny, nz, px, py, pz, CFL, fixed_dt)
+        self._init_initial_conditions(w0 if w0 is not None else Square(), w0_passives, conservative_ic, fv_ic,
+                                      progress_bar)
+        self._init_boundary_conditions(bc)
+        self._init_slope_limiting(a_posteriori_slope_limiting, slope_limiter, force_trouble, NAD, NAD_mode,
+                                  NAD_range, NAD_vars, PAD, SED, SED_tolerance, convex)
+        self._log_enabled = bool(log_troubles) and self.a_posteriori_slope_limiting
+        self._create_handle()
+        self._init_array_allocation()
+        self.timer.add_cat(
+            [
+                "boundary conditions",
+                "(high-order) hydrofluxes",
+                "(high-order) riemann solver",
+                "(high-order) conservative interpolation",
+                "(high-order) transverse reconstruction",
+                "(fallback scheme)",
+                "(fallback scheme) troubled cell detection",
+                "(fallback scheme) hydrofluxes",
+                "(fallback scheme) riemann solver",
+                "(fallback scheme) conservative interpolation",
+                "(fallback scheme) transverse reconstruction",
+            ]
+        )
+
+    # -- set-up (fvhoe/solver.py:220-420) ----------------------------------------
+    def _init_mesh(self, x, y, z, nx, ny, nz, px, py, pz, CFL, fixed_dt):
+        self.CFL = CFL
+        self.fixed_dt = fixed_dt
+        self.x_domain, self.y_domain, self.z_domain = x, y, z
+        self.h = ((x[1] - x[0]) / nx, (y[1] - y[0]) / ny, (z[1] - z[0]) / nz)
+        self.n = (nx, ny, nz)
+        self.p = (px, py, pz)
+        self.X, self.Y, self.Z = fv_uniform_meshgen(self.n, x, y, z)
+        self.x = self.X[:, 0, 0]
+        self.y = self.Y[0, :, 0]
+        self.z = self.Z[0, 0, :]
+        self.xdim = not (nx == 1 and px == 0)
+        self.ydim = not (ny == 1 and py == 0)
+        self.zdim = not (nz == 1 and pz == 0)
+        self.dims = "".join(d for d, on in zip("xyz", (self.xdim, self.ydim, self.zdim)) if on)
+        self.ndim = len(self.dims)
+
+    def _init_initial_conditions(self, w0, w0_passives, conservative_ic, fv_ic, progress_bar):
+        self.conservative_ic = conservative_ic
+        self.fv_ic = fv_ic
+        passives = tuple(w0_passives.keys()) if w0_passives is not None else ()
+        self.hydro_state = HydroState(passive_scalars=passives)
+        hs = self.hydro_state
+        self.nvars = hs.nvars
+        ic_func = w0.build_ic(hs, w0_passives)
+        if not {"x", "y", "z"}.issubset(inspect.signature(ic_func).parameters):
+            raise ValueError("Initial condition function must accept x, y, z as arguments.")
+        if conservative_ic and fv_ic:
+            self.w0 = NotImplemented
+            self.u0 = NotImplemented
+            self.u0_fv = ic_func
+        elif fv_ic:
+            raise ValueError("Can't have finite volume averages without conservative IC.")
+        else:
+            if conservative_ic:
+                self.w0 = NotImplemented
+                self.u0 = ic_func
+            else:
+                self.w0 = ic_func
+                self.u0 = lambda x, y, z: compute_conservatives(hs, ic_func(x, y, z), gamma=self.gamma)
+            self.u0_fv = lambda x, y, z: fv_average(self.u0, x, y, z, h=self.h, p=self.p)
+        u0 = np.ascontiguousarray(self.u0_fv(self.X, self.Y, self.Z), dtype=np.float64)
+        self._ode_init(progress_bar)
+        self.am = ArrayManager(backend="cuda")
+        self.am.add("u", u0)
+        self.f_evaluation_count = 0
+
+    def _init_boundary_conditions(self, bc):
+        if bc is None:
+            bc = BoundaryCondition(x="periodic", y="periodic", z="periodic")
+        self.bc = bc
+        self._bc_kinds = bc.kinds((self.xdim, self.ydim, self.zdim))
+
+    def _init_slope_limiting(self, a_posteriori_slope_limiting, slope_limiter, force_trouble, NAD, NAD_mode,
+                             NAD_range, NAD_vars, PAD, SED, SED_tolerance, convex):
+        self.a_posteriori_slope_limiting = a_posteriori_slope_limiting
+        self.slope_limiter = slope_limiter
+        self.force_trouble = force_trouble
+        self.NAD = NAD
+        self.NAD_mode = NAD_mode
+        self.NAD_range = NAD_range
+        self.NAD_vars = NAD_vars if isinstance(NAD_vars, tuple) or NAD_vars is None else tuple(NAD_vars)
+        self.PAD = {"rho": (0.0, np.inf), "P": (0.0, np.inf)} if PAD is None else PAD
+        self.SED = SED
+        self.SED_tolerance = SED_tolerance
+        self.convex = convex
+        self.trouble_counter = 1
+        if NAD_mode not in ("global", "local"):
+            raise ValueError(f"Unknown mode: {NAD_mode}")
+        if NAD_range not in ("relative", "absolute"):
+            raise ValueError(f"Unknown range_type: {NAD_range}")
+        if slope_limiter not in self._capi.LIMITER:
+            raise ValueError(f"Unknown slope limiter: {slope_limiter}")
+
+    def _config(self):
+        c = self._capi
+        cfg = c.default_config()
+        cfg.nvars = self.nvars
+        for a in range(3):
+            cfg.n[a] = self.n[a]
+            cfg.p[a] = self.p[a]
+            cfg.h[a] = self.h[a]
+            for side in range(2):
+                kind = self._bc_kinds[a][side]
+                cfg.bc[a][side] = c.BC.get(kind, 0) if kind is not None else 0
+        cfg.gamma = self.gamma
+        cfg.cfl = self.CFL
+        cfg.csq_floor = self.csq_floor
+        cfg.use_fixed_dt = 0 if self.fixed_dt is None else 1
+        cfg.fixed_dt = 0.0 if self.fixed_dt is None else float(self.fixed_dt)
+        cfg.riemann = c.RIEMANN[self.riemann_solver_name]
+        cfg.a_posteriori = int(bool(self.a_posteriori_slope_limiting))
+        cfg.slope_limiter = c.LIMITER[self.slope_limiter]
+        cfg.force_trouble = int(bool(self.force_trouble))
+        cfg.nad_eps = float(self.NAD)
+        cfg.nad_global = int(self.NAD_mode == "global")
+        cfg.nad_relative = int(self.NAD_range == "relative")
+        mask = 0x1F
+        if self.NAD_vars is not None:
+            mask = 0
+            for v in self.NAD_vars:
+                mask |= 1 << _VAR_INDEX[v]
+        cfg.nad_var_mask = mask
+        # only the last PAD entry takes effect, as in fvhoe/slope_limiting.py:229-237
+        if self.PAD:
+            var, (lo, hi) = list(self.PAD.items())[-1]
+            cfg.pad_var = _VAR_INDEX[var]
+            cfg.pad_lo = float(lo)
+            cfg.pad_hi = float(hi)
+        else:
+            cfg.pad_var = -1
+        cfg.sed = int(bool(self.SED))
+        cfg.sed_eps = float(self.SED_tolerance)
+        cfg.convex = int(bool(self.convex))
+        cfg.precision = c.PRECISION[self.precision]
+        cfg.log_troubles = int(self._log_enabled)
+        cfg.device = int(self.am("u").device.index or 0)
+        return cfg
+
+    def _create_handle(self):
+        import torch
+
+        c = self._capi
+        self._cfg = self._config()
+        handle = ctypes.c_void_p()
+        with torch.cuda.device(self.am("u").device):
+            c.check(c.lib.fvh_create(ctypes.byref(self._cfg), ctypes.byref(handle)))
+        self._handle = handle
+
+    def _init_array_allocation(self):
+        import torch
+
+        self.am.add("w", np.zeros((self.nvars,) + self.n))
+        self._dudt = None
+        self._log_tmp = torch.empty((3,) + self.n, dtype=torch.float64, device=self.am("u").device)
+
+    def __del__(self):
+        handle = getattr(self, "_handle", None)
+        if handle is not None and handle.value:
+            try:
+                self._capi.lib.fvh_destroy(handle)
+            except Exception:
+                pass
+            self._handle = None
+
+    # -- device calls -------------------------------------------------------------
+    def _stream(self):
+        import torch
+
+        return ctypes.c_void_p(torch.cuda.current_stream(self.am("u").device).cuda_stream)
+
+    def _as_device(self, u):
+        import torch
+
+        if isinstance(u, np.ndarray):
+            u = torch.from_numpy(np.ascontiguousarray(u, dtype=np.float64)).to(self.am("u").device)
+        if u.dtype != torch.float64 or not u.is_contiguous() or tuple(u.shape) != (self.nvars,) + self.n:
+            raise ValueError(f"u must be a contiguous float64 array of shape {(self.nvars,) + self.n}")
+        return u
+
+    def _set_log_mode(self):
+        if self._log_enabled:
+            self._capi.check(self._capi.lib.fvh_set_log_mode(self._handle, 1 if self.trouble_counter == 0 else 2),
+                             self._handle)
+
+    def f(self, t, u):
+        """One right-hand-side evaluation: (dt, dudt) (fvhoe/solver.py:422-454)."""
+        import torch
+
+        self.f_evaluation_count += 1
+        u = self._as_device(u)
+        dudt = torch.empty_like(u)
+        dt = ctypes.c_double()
+        self._set_log_mode()
+        self._capi.check(
+            self._capi.lib.fvh_rhs(self._handle, ctypes.c_void_p(u.data_ptr()), ctypes.c_void_p(dudt.data_ptr()),
+                                   ctypes.byref(dt), self._stream()),
+            self._handle,
+        )
+        if self._log_enabled:
+            self.trouble_counter += 1
+        return dt.value, dudt
+
+    def hydrodynamics(self, u):
+        return self.f(self.t, u)
+
+    def _device_step(self, integrator, target_time):
+        if integrator not in _STAGES:
+            raise ValueError(f"unknown integrator {integrator}")
+        u = self.am("u")
+        dt = ctypes.c_double()
+        self._set_log_mode()
+        self._capi.check(
+            self._capi.lib.fvh_step(
+                self._handle, ctypes.c_void_p(u.data_ptr()), self._capi.INTEGRATOR[integrator], float(self.t),
+                0 if target_time is None else 1, 0.0 if target_time is None else float(target_time),
+                ctypes.byref(dt), self._stream()),
+            self._handle,
+        )
+        self.f_evaluation_count += _STAGES[integrator]
+        if self._log_enabled:
+            self.trouble_counter += _STAGES[integrator]
+        return dt.value
+
+    def step_helper_function(self):
+        # log_troubles(reset=True) of fvhoe/solver.py:809-820
+        if self._log_enabled and self.trouble_counter > 0:
+            self._capi.check(
+                self._capi.lib.fvh_trouble_log(self._handle, float(self.trouble_counter), None, None, None,
+                                               self._stream()),
+                self._handle,
+            )
+            self.trouble_counter = 0
+
+    def trouble_flags(self) -> np.ndarray:
+        """Trouble flags (uint8, (nx, ny, nz)) of the last stage."""
+        import torch
+
+        out = torch.empty(self.n, dtype=torch.uint8, device=self.am("u").device)
+        self._capi.check(
+            self._capi.lib.fvh_trouble_flags(self._handle, ctypes.c_void_p(out.data_ptr()), self._stream()),
+            self._handle,
+        )
+        return out.cpu().numpy()
+
+    def stats(self) -> dict:
+        st = self._capi.FvhStats()
+        self._capi.check(self._capi.lib.fvh_get_stats(self._handle, ctypes.byref(st), self._stream()), self._handle)
+        return dict(dt_stage=st.dt_stage, dt_step=st.dt_step, troubled=st.troubled, nonfinite=st.nonfinite)
+
+    def primitives(self, u=None, fv_average: bool = True):
+        """FV-averaged (or cell-centre) primitives of u as a device tensor (fvhoe/solver.py:753-792)."""
+        import torch
+
+        u = self.am("u") if u is None else self._as_device(u)
+        w = torch.empty_like(u)
+        self._capi.check(
+            self._capi.lib.fvh_primitives(self._handle, ctypes.c_void_p(u.data_ptr()), ctypes.c_void_p(w.data_ptr()),
+                                          int(fv_average), self._stream()),
+            self._handle,
+        )
+        return w
+
+    def _trouble_logs(self):
+        t = self._log_tmp
+        self._capi.check(
+            self._capi.lib.fvh_trouble_log(self._handle, 0.0, ctypes.c_void_p(t[0].data_ptr()),
+                                           ctypes.c_void_p(t[1].data_ptr()), ctypes.c_void_p(t[2].data_ptr()),
+                                           self._stream()),
+            self._handle,
+        )
+        host = t.cpu().numpy()
+        return [np.broadcast_to(host[i], (5,) + self.n).copy() for i in range(3)]
+
+    # -- snapshots (fvhoe/solver.py:835-953) -----------------------------------------
+    def snapshot(self):
+        self.am("w").copy_(self.primitives(fv_average=self.snapshots_as_fv_averages))
+        log = {"x": self.x, "y": self.y, "z": self.z, "t": self.t, "w": self.am.get_numpy("w")}
+        if self.a_posteriori_slope_limiting:
+            if self._log_enabled:
+                trouble, nad, pad = self._trouble_logs()
+            else:
+                trouble = nad = pad = np.zeros((5,) + self.n)
+            log["trouble"] = trouble
+            log["NAD violation magnitude"] = nad
+            log["PAD violation magnitude"] = pad
+        self.snapshots.append(log)
+        self.snapshot_times.append(self.t)
+        if self.snapshot_helper_function is not None:
+            self.snapshot_helper_function(self)
+
+    def read_snapshots(self) -> bool:
+        if os.path.exists(self.snapshot_dir):
+            with open(os.path.join(self.snapshot_dir, "arrs.pkl"), "rb") as fh:
+                self.snapshots = pickle.load(fh)
+            print(f"Read from snapshot directory {self.snapshot_dir}")
+            return True
+        return False
+
+    def write_snapshots(self, overwrite: bool):
+        d = self.snapshot_dir
+        if os.path.exists(d) and not overwrite:
+            raise FileExistsError(f"Snapshot directory {d} already exists.")
+        if os.path.exists(d) and overwrite:
+            shutil.rmtree(d)
+            print(f"Clearing out snapshot directory {d}")
+        os.makedirs(d)
+        with open(os.path.join(d, "arrs.pkl"), "wb") as fh:
+            pickle.dump(self.snapshots, fh)
+        attrs = {}
+        for k, v in self.__dict__.items():
+            if k == "w0":
+                attrs[k] = getattr(v, "__name__", "__name__ not found")
+                continue
+            if k.startswith("_") or (callable(v) and k != "am") or isinstance(v, np.ndarray) or k in (
+                    "progress_bar", "timestamps", "snapshots", "w0_cell_centers_cache", "hydro_state"):
+                continue
+            if k in ("am", "bc", "timer"):
+                attrs[k] = v.to_dict()
+                continue
+            if k == "PAD":
+                attrs[k] = {key: [{np.inf: "inf", -np.inf: "-inf"}.get(i, i) for i in val] for key, val in v.items()}
+                continue
+            try:
+                json.dumps(v)
+            except TypeError:
+                continue
+            attrs[k] = v
+        attrs = {key: attrs[key] for key in sorted(attrs, key=lambda s: (s.lower(), s))}
+        with open(os.path.join(d, "attrs.json"), "w") as fh:
+            json.dump(attrs, fh, indent=4)
+        with open(os.path.join(d, "timing.txt"), "w") as fh:
+            fh.write(self.timer.report())
+        print(f"Wrote to snapshot directory {d}")
+
+    def run(self, *args, **kwargs):
+        """Runge-Kutta order from the degree, up to RK4 (fvhoe/solver.py:955-974)."""
+        q = min(max(self.p), 3)
+        return (self.euler, self.ssprk2, self.ssprk3, self.rk4)[q](*args, **kwargs)
+
+    def plot_1d_slice(self, *args, **kwargs):
+        raise NotImplementedError("plotting needs matplotlib, which this package does not use")
+
+    plot_2d_slice = plot_1d_slice
+    plot_fields = plot_1d_slice

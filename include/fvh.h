@@ -1,0 +1,203 @@
+/*
+ * fvh.h -- C ABI of the B200 per-stage update for the compressible Euler
+ * equations (high-order finite-volume reconstruction, HLLC/LLF/upwind Riemann
+ * fluxes, a-posteriori NAD/PAD troubled-cell detection with a MUSCL fallback,
+ * and SSP-RK stage accumulation).
+ *
+ * The library behind this header replaces the NumPy/CuPy hot path of
+ * jpalafou/FVHOE. Each entry point names the reference interface it stands in
+ * for (paths inside that project).
+ *
+ * Conventions
+ *  - Every call returns an int status: FVH_OK (0) or a negative FVH_ERR_*.
+ *    fvh_last_error() gives the message of the last failure (per handle, or
+ *    process-wide for fvh_create). No C++ exception crosses this boundary.
+ *  - State arrays are float64, layout (nvars, nx, ny, nz), C order (z
+ *    contiguous), exactly the reference's `u` (fvhoe/solver.py:410-420).
+ *    Pointers passed to the compute calls are DEVICE pointers; the caller
+ *    owns them. The library owns its scratch memory, allocated by fvh_create
+ *    and released by fvh_destroy.
+ *  - `stream` is a cudaStream_t passed as void*; NULL is the legacy default
+ *    stream. All work is ordered on that stream. Only the optional dt/host
+ *    read-backs synchronise it.
+ *  - A handle is not thread-safe; use one handle per solver and thread.
+ */
+#ifndef FVH_H
+#define FVH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FVH_ABI_VERSION 1
+
+/* status codes */
+#define FVH_OK 0
+#define FVH_ERR_CONFIG -1    /* invalid or unsupported configuration */
+#define FVH_ERR_CUDA -2      /* a CUDA runtime call failed */
+#define FVH_ERR_TIMEOUT -3   /* a bounded device-side wait gave up */
+#define FVH_ERR_NONFINITE -4 /* the update produced NaN/Inf values */
+#define FVH_ERR_ARG -5       /* invalid argument (null pointer, bad enum) */
+
+/* boundary kinds (fvhoe/boundary_conditions.py:357-373) */
+#define FVH_BC_PERIODIC 0
+#define FVH_BC_OUTFLOW 1 /* mirror */
+#define FVH_BC_REFLECTIVE 2 /* mirror, normal momentum negated */
+#define FVH_BC_FREE 3 /* repeat the edge cell */
+
+/* Riemann solvers (fvhoe/solver.py:185-193) */
+#define FVH_RIEMANN_HLLC 0
+#define FVH_RIEMANN_LLF 1
+#define FVH_RIEMANN_ADVECTION_UPWIND 2
+
+/* slope limiters of the fallback scheme (fvhoe/slope_limiting.py:40-48) */
+#define FVH_LIMITER_MINMOD 0
+#define FVH_LIMITER_MONCEN 1
+#define FVH_LIMITER_NONE 2
+
+/* precision modes */
+#define FVH_PREC_FP64 0 /* every operation in float64, reference evaluation order, no FMA contraction */
+#define FVH_PREC_FP32 1 /* reconstruction, Riemann fluxes, detection in float32; float64 stage accumulation */
+
+/* time integrators (fvhoe/ode.py:245-298) */
+#define FVH_INT_EULER 0
+#define FVH_INT_SSPRK2 1
+#define FVH_INT_SSPRK3 2
+#define FVH_INT_RK4 3
+
+typedef struct fvh_config {
+  int abi_version;   /* FVH_ABI_VERSION */
+  int nvars;         /* 5 + number of passive scalars (<= 16) */
+  int n[3];          /* cells along x, y, z; an axis with n = 1 and p = 0 is inactive */
+  int p[3];          /* polynomial degree per axis, 0..8 */
+  double h[3];       /* cell widths */
+  double gamma;      /* specific heat ratio */
+  double cfl;        /* Courant number */
+  double csq_floor;  /* floor on the squared sound speed */
+  int use_fixed_dt;  /* 1: use fixed_dt instead of the CFL step */
+  double fixed_dt;
+  int riemann;       /* FVH_RIEMANN_* */
+  int bc[3][2];      /* FVH_BC_* at the low/high end of each axis */
+  int a_posteriori;  /* 1: NAD/PAD detection with the fallback scheme */
+  int slope_limiter; /* FVH_LIMITER_* */
+  int force_trouble; /* 1: every cell is troubled */
+  double nad_eps;    /* NAD tolerance */
+  int nad_global;    /* 1: "global" range, 0: "local" */
+  int nad_relative;  /* 1: "relative" range, 0: "absolute" */
+  int nad_var_mask;  /* bit v (0..4) set: primitive v takes part in NAD */
+  int pad_var;       /* primitive index checked by PAD, or -1 for none */
+  double pad_lo;
+  double pad_hi;
+  int sed;           /* 1: smooth-extrema detection relaxes NAD */
+  double sed_eps;
+  int convex;        /* 1: convex face weights (1D/2D only) */
+  int precision;     /* FVH_PREC_* */
+  int log_troubles;  /* 1: keep the running trouble / NAD / PAD sums used by snapshots */
+  int device;        /* CUDA device ordinal the handle's memory and kernels live on */
+} fvh_config;
+
+typedef struct fvh_handle fvh_handle;
+
+/* Stage statistics of the last call. */
+typedef struct fvh_stats {
+  double dt_stage;       /* dt of the last stage (CFL or fixed) */
+  double dt_step;        /* dt of the last step after the target clamp */
+  unsigned int troubled; /* troubled cells in the last stage */
+  unsigned int nonfinite;/* non-finite values written by the last stage */
+} fvh_stats;
+
+/* Fills *cfg with the reference's defaults (fvhoe/solver.py:42-84):
+ * gamma 5/3, CFL 0.8, HLLC, periodic, NAD 1e-2 global relative on all
+ * variables, PAD on P >= 0 (the last key of the default PAD dict), SED on
+ * with tolerance 1e-10, minmod, csq_floor 1e-10, FP64. */
+void fvh_config_default(fvh_config* cfg);
+
+/* Validates cfg and allocates the scratch memory of one solver on the current
+ * CUDA device. Replaces the array allocation of EulerSolver.__init__
+ * (fvhoe/solver.py:402-420) for the "cuda" backend. */
+int fvh_create(const fvh_config* cfg, fvh_handle** out);
+
+/* Releases a handle and its scratch memory. NULL is accepted. */
+int fvh_destroy(fvh_handle* h);
+
+/* Message of the last failure on h, or of the last failed fvh_create when h
+ * is NULL. Never NULL. */
+const char* fvh_last_error(const fvh_handle* h);
+
+/* Bytes of device scratch memory held by the handle. */
+size_t fvh_scratch_bytes(const fvh_handle* h);
+
+/* One right-hand-side evaluation: dudt = L(u) and the CFL time step of this
+ * evaluation. Replaces EulerSolver.f / hydrodynamics (fvhoe/solver.py:422-454)
+ * including revise_fluxes (:653-732) and euler_equation (:734-751).
+ * u, dudt: device arrays of nvars * nx * ny * nz doubles. dt_out: host
+ * pointer or NULL; when given, the call synchronises the stream. */
+int fvh_rhs(fvh_handle* h, const double* u, double* dudt, double* dt_out, void* stream);
+
+/* One time step of the chosen integrator, updating u in place. The first
+ * stage's dt is shortened to target - t when has_target is set and the target
+ * is closer (fvhoe/ode.py:11-22). Replaces ODE.take_step with the stepper of
+ * ODE.euler/ssprk2/ssprk3/rk4 (fvhoe/ode.py:183-193, 245-298).
+ * dt_out: host pointer or NULL (when given, the stream is synchronised). */
+int fvh_step(fvh_handle* h, double* u, int integrator, double t, int has_target, double target, double* dt_out,
+             void* stream);
+
+/* Finite-volume primitive averages (fv_average = 1) or cell-centre primitives
+ * (fv_average = 0) of u over the interior, written to w (same shape).
+ * Replaces interpolate_primitives_from_conservatives with gw = 0
+ * (fvhoe/solver.py:753-792) as called by snapshot (:840-874). */
+int fvh_primitives(fvh_handle* h, const double* u, double* w, int fv_average, void* stream);
+
+/* Copies the trouble flags of the last stage (uint8, nx*ny*nz) to the device
+ * array flags. Replaces the troubled_cells array of revise_fluxes
+ * (fvhoe/solver.py:691-706). */
+int fvh_trouble_flags(fvh_handle* h, uint8_t* flags, void* stream);
+
+/* Running trouble / NAD / PAD sums of log_troubles (fvhoe/solver.py:794-833).
+ * divide_by > 0 divides the sums in place first (the reset branch of
+ * log_troubles); each destination may be NULL. Destinations are device arrays
+ * of nx*ny*nz doubles. */
+int fvh_trouble_log(fvh_handle* h, double divide_by, double* trouble, double* nad_mag, double* pad_mag,
+                    void* stream);
+
+/* Selects how the next stage writes the trouble log: 1 overwrites the sums,
+ * 2 adds to them (the two branches of log_troubles, fvhoe/solver.py:821-833). */
+int fvh_set_log_mode(fvh_handle* h, int mode);
+
+/* Statistics of the last stage; synchronises the stream. */
+int fvh_get_stats(fvh_handle* h, fvh_stats* out, void* stream);
+
+/* Kernel kinds reported by fvh_profile_read. The per-launch timing replaces
+ * the wall-clock categories of the reference's Timer (fvhoe/timer.py:6-109,
+ * categories registered at fvhoe/solver.py:204-218). */
+#define FVH_KK_CENTRE 0     /* centre-interpolation sweeps (ghost fill, primitives) */
+#define FVH_KK_TRANSVERSE 1 /* transverse-reconstruction sweeps (CFL / extrema reductions) */
+#define FVH_KK_FACE 2       /* face states + Riemann solve */
+#define FVH_KK_CANDIDATE 3  /* unlimited candidate update */
+#define FVH_KK_DETECT 4     /* troubled-cell detection */
+#define FVH_KK_FALLBACK 5   /* MUSCL fallback + blend */
+#define FVH_KK_FINAL 6      /* flux divergence + Runge-Kutta combination */
+#define FVH_KK_SMALL 7      /* stage scalars, convex weights, log arithmetic */
+#define FVH_KK_COUNT 8
+
+/* Total kernel launches issued by this library in this process. */
+uint64_t fvh_kernel_launches(void);
+
+/* on = 1: time every launch made for h with a CUDA event pair (a few
+ * microseconds of overhead per launch); on = 0: stop timing. */
+int fvh_profile_enable(fvh_handle* h, int on);
+
+/* Synchronises the stream, then writes per kernel kind (arrays of
+ * FVH_KK_COUNT, each may be NULL) the milliseconds, the bytes each launch must
+ * move (inputs read once, outputs written once) and the launch counts
+ * accumulated since the previous read, and clears them. */
+int fvh_profile_read(fvh_handle* h, double* ms, double* bytes, uint64_t* launches, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FVH_H */
