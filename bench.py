@@ -1,0 +1,385 @@
+"""Benchmark: Mcell-updates/s of FVHOE's per-stage update on B200.
+
+Workload: 2D Kelvin-Helmholtz, periodic unit square, 2048^2 cells, gamma 1.4,
+p = 5, HLLC, SSP-RK3, CFL 0.8, a-posteriori NAD (1e-5, global relative) + PAD
+with SED and the MUSCL/minmod fallback; the initial state is the seeded
+synthetic KH band with per-cell vy noise of amplitude 1e-3. One bench step is
+one SSP-RK3 step (3 stages), i.e. 3 * 2048^2 cell-updates, the reference's
+own unit (cells x RK stages / time).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|fp32]
+  python bench.py --impl reference ...   # the reference algorithm on the host cores
+
+With N > 1 (launched by torch.distributed.run) every rank advances its own
+replica (a different noise seed); there is no data-path collective, the
+timing is the maximum over ranks and `value` counts the cells of all ranks.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-updates/s on 1 B200: chosen form vs plain FP64 at stated L1 error"
+UNIT = "Mcell-updates/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--n", type=int, default=2048, help="cells per side")
+    ap.add_argument("--p", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-sample", type=int, default=512, help="side of the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(args, n=None):
+    n = args.n if n is None else n
+    return {
+        "workload": f"2D Kelvin-Helmholtz {n}x{n}, p={args.p}, HLLC, SSP-RK3, CFL 0.8, "
+                    "a-posteriori NAD 1e-5 + PAD + SED, MUSCL-minmod fallback, periodic",
+        "cells": n * n,
+        "p": args.p,
+        "riemann": "hllc",
+        "integrator": "ssprk3",
+        "precision": args.precision,
+        "step": "one SSP-RK3 step = 3 stages = 3 cell-updates per cell",
+        "l2": "inputs larger than L2: the float64 state alone is 5*8*n^2 bytes",
+    }
+
+
+def solver_kwargs(n, p, seed):
+    from fvhoe_b200 import KelvinHelmholtzNoise2D
+
+    return dict(w0=KelvinHelmholtzNoise2D(n=(n, n), seed=seed), nx=n, ny=n, px=p, py=p, gamma=1.4,
+                riemann_solver="hllc", CFL=0.8, a_posteriori_slope_limiting=True, NAD=1e-5, progress_bar=False)
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (one process per GPU)
+# ---------------------------------------------------------------------------
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        if args.impl == "reference":
+            return rank, world, local, None
+        import torch
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        return rank, world, local, dist
+    return rank, world, local, None
+
+
+def max_over_ranks(x, dist):
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"fvh_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu)], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for name, val in zip(names, parts[5:9]):
+                    if val.lower() == "active":
+                        reasons.add(name)
+        os.remove(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(kind, n, p, precision):
+    """DRAM bytes per launch of `kind` from the committed ncu summary, scaled to n^2 cells."""
+    path = os.path.join(ROOT, "profiles", "traffic_kh_per_launch.json")
+    try:
+        with open(path) as fh:
+            data = json.load(fh)
+        rec = data[f"{precision}_p{p}"][kind]
+        return rec["bytes_per_launch"] * (n * n) / rec["cells"]
+    except (OSError, KeyError, ValueError, TypeError):
+        return None
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines (the oracle port of the reference algorithm)
+# ---------------------------------------------------------------------------
+def _oracle_sample(job):
+    """One SSP-RK3 step of the KH workload on an n x n sample with the oracle; returns seconds."""
+    n, p, seed = job
+    import numpy as np
+
+    sys.path.insert(0, ROOT)
+    from fvhoe_b200.fv import fv_average, fv_uniform_meshgen
+    from fvhoe_b200.hydro import HydroState, compute_conservatives
+    from fvhoe_b200.initial_conditions import KelvinHelmholtzNoise2D
+    from oracle import fvh_oracle as O
+
+    hs = HydroState()
+    f = KelvinHelmholtzNoise2D(n=(n, n), seed=seed).build_ic(hs)
+    X, Y, Z = fv_uniform_meshgen((n, n, 1))
+    h = (1 / n, 1 / n, 1.0)
+    u0 = fv_average(lambda x, y, z: compute_conservatives(hs, f(x, y, z), 1.4), X, Y, Z, h=h, p=(p, p, 0))
+    cfg = O.OracleConfig(n=(n, n, 1), p=(p, p, 0), h=h, gamma=1.4, riemann_solver="hllc", CFL=0.8,
+                         a_posteriori_slope_limiting=True, NAD=1e-5)
+    t0 = time.perf_counter()
+    O.step(np.ascontiguousarray(u0), 0.0, cfg, "ssprk3")
+    return time.perf_counter() - t0
+
+
+def cpu_baseline_port(args):
+    n = args.cpu_sample
+    sec = _oracle_sample((n, args.p, 0))
+    return {"value": 3 * n * n / sec / 1e6, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"one SSP-RK3 step of the same KH workload at {n}x{n} (p={args.p}) with the NumPy "
+                      f"oracle (single-threaded NumPy, 1 core of {os.cpu_count()}); {sec:.1f} s"}
+
+
+def run_reference(args):
+    """The reference algorithm (the oracle port; the reference is pure Python and cannot be
+    installed on the GPU host) on all host cores: each bench step runs one SSP-RK3 step of
+    independent KH samples in parallel processes."""
+    import multiprocessing as mp
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    side = 128 if args.steps > 30 else 192
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        for _ in range(args.warmup):
+            pool.map(_oracle_sample, [(side, args.p, i) for i in range(cores)])
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            pool.map(_oracle_sample, [(side, args.p, k * cores + i) for i in range(cores)])
+        wall = time.perf_counter() - t0
+    cell_updates = 3 * side * side * cores * args.steps
+    value = cell_updates / wall / 1e6
+    sample = (f"per bench step: {cores} processes each run one SSP-RK3 step of the KH workload at "
+              f"{side}x{side} (p={args.p}) with the NumPy oracle port of the reference")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(args),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    rank, world, local, dist = dist_setup(args)
+    torch.cuda.set_device(local)
+    from fvhoe_b200 import EulerSolver, _capi
+
+    lib = _capi.lib
+    s = EulerSolver(precision=args.precision, **solver_kwargs(args.n, args.p, seed=rank))
+    h = s._handle
+    u = s.am("u")
+    stream = torch.cuda.current_stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    uptr = ctypes.c_void_p(u.data_ptr())
+    ssprk3 = _capi.INTEGRATOR["ssprk3"]
+    cells = args.n * args.n
+
+    def step():
+        # one SSP-RK3 step exactly as EulerSolver.take_step issues it, minus the dt read-back:
+        # the trouble log restarts, three stages accumulate into it, the step divides it by 3
+        _capi.check(lib.fvh_set_log_mode(h, 1), h)
+        _capi.check(lib.fvh_step(h, uptr, ssprk3, 0.0, 0, 0.0, None, sp), h)
+        _capi.check(lib.fvh_trouble_log(h, 3.0, None, None, None, sp), h)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # timed region (device-resident state)
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = lib.fvh_kernel_launches()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = lib.fvh_kernel_launches() - l0
+    ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = max_over_ranks(ms, dist)
+    value = world * 3 * cells * args.steps / (ms / 1e3) / 1e6
+
+    # per-kernel timing of a few steps for the roofline of the dominant kernel
+    _capi.check(lib.fvh_profile_enable(h, 1), h)
+    prof_steps = 3
+    for _ in range(prof_steps):
+        step()
+    K = len(_capi.KERNEL_KINDS)
+    pms = (ctypes.c_double * K)()
+    pbytes = (ctypes.c_double * K)()
+    plaunch = (ctypes.c_uint64 * K)()
+    _capi.check(lib.fvh_profile_read(h, pms, pbytes, plaunch, sp), h)
+    _capi.check(lib.fvh_profile_enable(h, 0), h)
+    total_ms = sum(pms)
+    kinds = {}
+    for i, name in enumerate(_capi.KERNEL_KINDS):
+        if plaunch[i]:
+            kinds[name] = {"ms_per_step": pms[i] / prof_steps, "share": pms[i] / total_ms,
+                           "launches_per_step": plaunch[i] / prof_steps,
+                           "gb_s": pbytes[i] / (pms[i] / 1e3) / 1e9 if pms[i] > 0 else None}
+    dom = max(range(K), key=lambda i: pms[i])
+    dom_name = _capi.KERNEL_KINDS[dom]
+    per_launch_bytes = pbytes[dom] / plaunch[dom]
+    per_launch_s = pms[dom] / plaunch[dom] / 1e3
+    achieved = per_launch_bytes / per_launch_s / 1e9
+    peak, peak_src = hbm_peak()
+    traffic = ncu_traffic(dom_name, args.n, args.p, args.precision)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": dom_name, "peak_source": f"{peak_src} HBM copy bandwidth",
+                "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_s * 1e3,
+                "stage_model": {"bytes_per_cell_update": 120,
+                                "achieved_gb_s": 120 * value / world * 1e6 / 1e9}}
+
+    # end to end through the C ABI with host buffers: per step, copy the state in from
+    # pinned host memory, run the step with its dt read-back, copy the state out
+    host = torch.empty(u.shape, dtype=torch.float64, pin_memory=True)
+    host.copy_(u)
+    torch.cuda.synchronize()
+    nbytes = u.numel() * 8
+    dt = ctypes.c_double()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        u.copy_(host, non_blocking=True)
+        _capi.check(lib.fvh_set_log_mode(h, 1), h)
+        _capi.check(lib.fvh_step(h, uptr, ssprk3, 0.0, 0, 0.0, ctypes.byref(dt), sp), h)
+        _capi.check(lib.fvh_trouble_log(h, 3.0, None, None, None, sp), h)
+        host.copy_(u, non_blocking=True)
+        stream.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(e2e_s, dist)
+    e2e = {"value": world * 3 * cells * args.e2e_steps / e2e_s / 1e6, "unit": UNIT,
+           "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": args.e2e_steps,
+           "path": "fvh_step through the C ABI; state copied from/to pinned host memory every step"}
+
+    stats = s.stats()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32", "data": "synthetic",
+            "config": dict(workload_config(args), parallelism=f"replicas x{world}" if world > 1 else "single"),
+            "chosen_form": f"plain {args.precision} (generic multi-pass kernels)",
+            "l1_density_error_vs_fp64": 0.0 if args.precision == "fp64" else None,
+            "roofline": roofline, "kernels": kinds, "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
+            "troubled_cells_last_stage": stats["troubled"], "nonfinite": stats["nonfinite"],
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_port(args)
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

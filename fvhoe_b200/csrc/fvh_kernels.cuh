@@ -259,21 +259,50 @@ __global__ void __launch_bounds__(256) k_transverse_sweep(const Tc* __restrict__
     }
   }
   if constexpr (REDUCE) {
-    const bool lead = (threadIdx.x & 31) == 0;
-    if (rs.cfl) {
-      cfl_key = warp_max_u64(cfl_key);
-      if (lead && cfl_key) atomicMax(&sc->cfl_key, cfl_key);
+    // warp, then block reduction in shared memory: one atomic per key and block
+    __shared__ unsigned long long s_keys[8][11];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned long long c = warp_max_u64(cfl_key);
+    if (lane == 0) s_keys[warp][0] = c;
+    for (int v = 0; v < 5; ++v) {
+      const unsigned long long a = warp_max_u64(kmax[v]);
+      const unsigned long long b = warp_min_u64(kmin[v]);
+      if (lane == 0) {
+        s_keys[warp][1 + v] = a;
+        s_keys[warp][6 + v] = b;
+      }
     }
-    if (rs.extrema) {
-      for (int v = 0; v < 5; ++v) {
-        const unsigned long long a = warp_max_u64(kmax[v]);
-        const unsigned long long b = warp_min_u64(kmin[v]);
-        if (lead) {
-          if (a) atomicMax(&sc->vmax_key[v], a);
-          if (b != ~0ull) atomicMin(&sc->vmin_key[v], b);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int nw = blockDim.x >> 5;
+      unsigned long long acc[11];
+      for (int k = 0; k < 11; ++k) acc[k] = s_keys[0][k];
+      for (int w = 1; w < nw; ++w) {
+        for (int k = 0; k < 6; ++k) acc[k] = s_keys[w][k] > acc[k] ? s_keys[w][k] : acc[k];
+        for (int k = 6; k < 11; ++k) acc[k] = s_keys[w][k] < acc[k] ? s_keys[w][k] : acc[k];
+      }
+      if (rs.cfl && acc[0]) atomicMax(&sc->cfl_key, acc[0]);
+      if (rs.extrema) {
+        for (int v = 0; v < 5; ++v) {
+          if (acc[1 + v]) atomicMax(&sc->vmax_key[v], acc[1 + v]);
+          if (acc[6 + v] != ~0ull) atomicMin(&sc->vmin_key[v], acc[6 + v]);
         }
       }
     }
+  }
+}
+
+// Block-wide sum of a per-thread count with one atomic per block (blocks of
+// at most 256 threads).
+__device__ __forceinline__ void block_count_add(unsigned int count, unsigned int* dst) {
+  __shared__ unsigned int s_count[8];
+  for (int o = 16; o > 0; o >>= 1) count += __shfl_xor_sync(0xffffffffu, count, o);
+  if ((threadIdx.x & 31) == 0) s_count[threadIdx.x >> 5] = count;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int total = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) total += s_count[w];
+    if (total) atomicAdd(dst, total);
   }
 }
 
@@ -479,8 +508,7 @@ __global__ void __launch_bounds__(256) k_detect(const Tc* __restrict__ w, Region
       }
     }
   }
-  for (int o = 16; o > 0; o >>= 1) count += __shfl_xor_sync(0xffffffffu, count, o);
-  if ((threadIdx.x & 31) == 0 && count) atomicAdd(&sc->troubled, count);
+  block_count_add(count, &sc->troubled);
 }
 
 // ---------------------------------------------------------------------------
@@ -655,8 +683,7 @@ __global__ void __launch_bounds__(256) k_final(Region rint, FluxSet fs, Phys<Tc>
       bad += isfinite(res) ? 0u : 1u;
     }
   }
-  for (int o = 16; o > 0; o >>= 1) bad += __shfl_xor_sync(0xffffffffu, bad, o);
-  if ((threadIdx.x & 31) == 0 && bad) atomicAdd(&sc->nonfinite, bad);
+  block_count_add(bad, &sc->nonfinite);
 }
 
 // ---------------------------------------------------------------------------

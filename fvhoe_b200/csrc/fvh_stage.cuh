@@ -203,7 +203,8 @@ template <typename Tc, int NV, int K>
 void launch_transverse_k(bool reduce, const Tc* in, Region rin, Tc* out, Region rout, int axis, const HostRule& hr,
                          const Phys<Tc>& ph, const ReduceSpec& rs, Scalars* sc, cudaStream_t s) {
   const Rule<Tc, K> rule = device_rule<Tc, K>(hr);
-  const unsigned nb = blocks_for(region_points(rout));
+  // reducing sweeps use a bounded, grid-stride grid so each block folds many points
+  const unsigned nb = reduce ? std::min(blocks_for(region_points(rout)), 148u * 8u) : blocks_for(region_points(rout));
   LaunchScope scope(KK_TRANSVERSE,
                     region_bytes(rout, ph.nv, sizeof(Tc), axis, K - 1) + region_bytes(rout, ph.nv, sizeof(Tc)), s);
   if (reduce)

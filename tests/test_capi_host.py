@@ -1,0 +1,189 @@
+"""C ABI and host-side logic without a GPU.
+
+The library must load and export every symbol include/fvh.h declares; its
+configuration checks run on the host before any device work; the Python host
+classes keep the reference's interfaces and errors.
+"""
+
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _header_functions():
+    text = open(os.path.join(ROOT, "include", "fvh.h")).read()
+    return sorted(set(re.findall(r"\b(fvh_[a-z_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_function():
+    from fvhoe_b200 import _capi
+
+    declared = _header_functions()
+    assert len(declared) >= 12
+    missing = [name for name in declared if not hasattr(_capi.lib, name)]
+    assert not missing, missing
+    assert set(declared) == set(_capi.EXPORTS)
+
+
+def test_config_struct_layout_matches_header(tmp_path):
+    from fvhoe_b200 import _capi
+
+    src = tmp_path / "size.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "fvh.h"\n'
+                   'int main(){printf("%zu %zu %zu %zu\\n", sizeof(fvh_config), offsetof(fvh_config, device),'
+                   ' offsetof(fvh_config, pad_hi), sizeof(fvh_stats));return 0;}\n')
+    exe = tmp_path / "size"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    size, dev, pad_hi, stats = map(int, subprocess.run([str(exe)], capture_output=True, text=True).stdout.split())
+    assert size == ctypes.sizeof(_capi.FvhConfig)
+    assert dev == _capi.FvhConfig.device.offset
+    assert pad_hi == _capi.FvhConfig.pad_hi.offset
+    assert stats == ctypes.sizeof(_capi.FvhStats)
+
+
+def test_default_config_matches_reference_defaults():
+    from fvhoe_b200 import _capi
+
+    c = _capi.default_config()
+    assert c.abi_version == _capi.ABI_VERSION and c.nvars == 5
+    assert c.gamma == 5 / 3 and c.cfl == 0.8 and c.csq_floor == 1e-10
+    assert c.riemann == _capi.RIEMANN["hllc"] and c.slope_limiter == _capi.LIMITER["minmod"]
+    assert c.nad_eps == 1e-2 and c.nad_global == 1 and c.nad_relative == 1 and c.nad_var_mask == 0x1F
+    assert c.pad_var == 4 and c.pad_lo == 0.0 and c.pad_hi == float("inf")
+    assert c.sed == 1 and c.sed_eps == 1e-10
+    assert list(c.bc[0]) == [0, 0]
+
+
+@pytest.mark.parametrize(
+    "change, message",
+    [
+        (dict(p=(9, 0, 0)), "p must be in [0, 8]"),
+        (dict(n=(8, 1, 1), p=(5, 0, 0)), "fewer than the 12 ghost cells"),
+        (dict(nvars=4), "nvars must be in [5, 16]"),
+        (dict(riemann=7), "unknown Riemann solver"),
+        (dict(bc=((1, 0), (0, 0), (0, 0))), "periodic high boundary"),
+        (dict(n=(1, 1, 1), p=(0, 0, 0)), "no active axis"),
+        (dict(a_posteriori=1, convex=1, n=(32, 32, 32), p=(1, 1, 1)), "3D convex"),
+        (dict(pad_var=7), "pad_var"),
+    ],
+)
+def test_create_refuses_bad_configs_before_device_work(change, message):
+    from fvhoe_b200 import _capi
+
+    c = _capi.default_config()
+    c.n[0], c.p[0] = 64, 3
+    for key, val in change.items():
+        if key in ("n", "p"):
+            for a in range(3):
+                getattr(c, key)[a] = val[a]
+        elif key == "bc":
+            for a in range(3):
+                c.bc[a][0], c.bc[a][1] = val[a]
+        else:
+            setattr(c, key, val)
+    h = ctypes.c_void_p()
+    st = _capi.lib.fvh_create(ctypes.byref(c), ctypes.byref(h))
+    assert st == _capi.ERR_CONFIG
+    assert message in _capi.lib.fvh_last_error(None).decode()
+    assert not h.value
+
+
+def test_null_arguments_are_refused():
+    from fvhoe_b200 import _capi
+
+    assert _capi.lib.fvh_create(None, None) == _capi.ERR_ARG
+    assert _capi.lib.fvh_rhs(None, None, None, None, None) == _capi.ERR_ARG
+    assert _capi.lib.fvh_destroy(None) == _capi.OK
+    assert _capi.lib.fvh_scratch_bytes(None) == 0
+
+
+def test_hydrostate_slices_like_reference():
+    from fvhoe_b200 import HydroState
+
+    hs = HydroState(passive_scalars=("a", "b"))
+    assert hs.nvars == 7 and hs("rho") == (0, slice(None), slice(None), slice(None))
+    assert hs(x=(1, -1))[1] == slice(1, -1)
+    assert list(hs("passive_scalars")[0]) == [5, 6]
+    assert HydroState(ndim=1)("P") == 4
+    with pytest.raises(ValueError):
+        hs("nope")
+    with pytest.raises(ValueError):
+        HydroState(passive_scalars=("a", "a"))
+
+
+def test_boundary_condition_parsing_and_refusals():
+    from fvhoe_b200 import BoundaryCondition
+
+    bc = BoundaryCondition(x=("reflective", "outflow"), y="free")
+    assert bc.x == ("reflective", "outflow") and bc.y == ("free", "free") and bc.z == ("periodic", "periodic")
+    assert bc.kinds((True, True, False))[0] == ("reflective", "outflow")
+    with pytest.raises(NotImplementedError):
+        BoundaryCondition(x="dirichlet").kinds((True, False, False))
+    with pytest.raises(ValueError):
+        BoundaryCondition(x=("outflow", "periodic")).kinds((True, False, False))
+    with pytest.raises(ValueError):
+        BoundaryCondition(x=["outflow", "outflow"])
+
+
+def test_array_manager_errors_like_reference():
+    from fvhoe_b200 import ArrayManager
+
+    am = ArrayManager()
+    am.add("u", np.zeros(3))
+    with pytest.raises(KeyError):
+        am.add("u", np.zeros(3))
+    with pytest.raises(TypeError):
+        am.add("v", [1, 2, 3])
+    with pytest.raises(KeyError):
+        am("missing")
+    assert am.to_dict()["names"] == ["u"]
+    got = am.get_numpy("u")
+    got[0] = 5
+    assert am("u")[0] == 0
+    am.remove("u")
+    with pytest.raises(KeyError):
+        am.get_numpy("u")
+
+
+def test_timer_categories():
+    from fvhoe_b200 import Timer
+
+    t = Timer(cats=["TOTAL"])
+    t.start("TOTAL")
+    with pytest.raises(RuntimeError):
+        t.start("TOTAL")
+    t.stop("TOTAL")
+    with pytest.raises(ValueError):
+        t.add_cat("TOTAL")
+    assert "TOTAL" in t.report()
+
+
+def test_initial_conditions_match_oracle_setup():
+    """The package's FV-averaged initial states equal those the fixtures were made from."""
+    from fvhoe_b200.fv import fv_average, fv_uniform_meshgen
+    from fvhoe_b200.hydro import HydroState, compute_conservatives
+    from fvhoe_b200.initial_conditions import KelvinHelmholtzNoise2D, SedovBlast, Shock1D
+    from tests.fixtures import GOLDEN, load
+
+    hs = HydroState()
+    c, d = load(os.path.join(GOLDEN, "steps_sod_full.npz"))
+    X, Y, Z = fv_uniform_meshgen((256, 1, 1))
+    f = Shock1D().build_ic(hs)
+    u0 = fv_average(lambda x, y, z: compute_conservatives(hs, f(x, y, z), 1.4), X, Y, Z, h=tuple(c["h"]),
+                    p=(3, 0, 0))
+    assert np.array_equal(u0, d["u0"])
+    c, d = load(os.path.join(GOLDEN, "steps_kh64_p5.npz"))
+    X, Y, Z = fv_uniform_meshgen((64, 64, 1))
+    f = KelvinHelmholtzNoise2D(n=(64, 64), seed=7).build_ic(hs)
+    u0 = fv_average(lambda x, y, z: compute_conservatives(hs, f(x, y, z), 1.4), X, Y, Z, h=tuple(c["h"]),
+                    p=(5, 5, 0))
+    assert np.array_equal(u0, d["u0"])
+    c, d = load(os.path.join(GOLDEN, "steps_sedov3d16_p3.npz"))
+    X, Y, Z = fv_uniform_meshgen((16, 16, 16))
+    assert np.array_equal(SedovBlast(dims="xyz").build_ic(hs)(X, Y, Z), d["u0"])
