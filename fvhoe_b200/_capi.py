@@ -43,6 +43,9 @@ EXPORTS = (
     "fvh_kernel_launches",
     "fvh_profile_enable",
     "fvh_profile_read",
+    "fvh_primitives_noalloc",
+    "fvh_primitives_noalloc_max_doubles",
+    "fvh_primitives_noalloc_error",
 )
 
 KERNEL_KINDS = ("centre", "transverse", "face", "candidate", "detect", "fallback", "final", "small")
@@ -122,6 +125,12 @@ def _load():
     lib.fvh_kernel_launches.restype = ctypes.c_uint64
     lib.fvh_profile_enable.argtypes = [vp, ctypes.c_int]
     lib.fvh_profile_read.argtypes = [vp, dp, dp, ctypes.POINTER(ctypes.c_uint64), vp]
+    lib.fvh_primitives_noalloc.argtypes = [ctypes.POINTER(FvhConfig), vp, vp, ctypes.c_int, vp]
+    lib.fvh_primitives_noalloc.restype = ctypes.c_int
+    lib.fvh_primitives_noalloc_max_doubles.argtypes = []
+    lib.fvh_primitives_noalloc_max_doubles.restype = ctypes.c_size_t
+    lib.fvh_primitives_noalloc_error.argtypes = []
+    lib.fvh_primitives_noalloc_error.restype = ctypes.c_char_p
     for name in ("fvh_create", "fvh_destroy", "fvh_rhs", "fvh_step", "fvh_primitives", "fvh_trouble_flags",
                  "fvh_trouble_log", "fvh_set_log_mode", "fvh_get_stats", "fvh_profile_enable", "fvh_profile_read"):
         getattr(lib, name).restype = ctypes.c_int

@@ -31,6 +31,7 @@ UNITS = {
     "fvh_api.cu": [],
     "fvh_stage_f64.cu": ["-fmad=false"],
     "fvh_stage_f32.cu": ["-fmad=true"],
+    "fvh_noalloc.cu": ["-fmad=false"],
 }
 
 

@@ -298,6 +298,15 @@ int allocate(fvh_handle* h) {
   return FVH_OK;
 }
 
+}  // namespace
+
+namespace fvh {
+// Configuration checks shared with the handle-free entry point (fvh_noalloc.cu).
+int configure_handle(fvh_handle* h, const fvh_config* cfg, std::string& msg) { return configure(h, cfg, msg); }
+}  // namespace fvh
+
+namespace {
+
 int run_stage(fvh_handle* h, const fvh::StageCall& c, cudaStream_t s) {
   ProfilerBinding bind(h);
   return h->cfg.precision == FVH_PREC_FP32 ? fvh::run_stage_f32(h, c, s) : fvh::run_stage_f64(h, c, s);

@@ -151,6 +151,21 @@ int fvh_step(fvh_handle* h, double* u, int integrator, double t, int has_target,
  * (fvhoe/solver.py:753-792) as called by snapshot (:840-874). */
 int fvh_primitives(fvh_handle* h, const double* u, double* w, int fv_average, void* stream);
 
+/* Allocation-free fvh_primitives, with no counterpart in the reference. For
+ * callers that cannot allocate device memory when they convert (a host
+ * application owning the device memory pool, or a run that has committed the
+ * whole device to its state): no handle, no cudaMalloc; the two sweep buffers
+ * come from a 16 MiB static device array that every GPU loading this library
+ * holds until exit. cfg is checked as by fvh_create; grids needing more than
+ * fvh_primitives_noalloc_max_doubles() doubles per buffer
+ * (nvars * prod(n_a + 4 ceil(p_a/2)) over the active axes) are refused with
+ * FVH_ERR_CONFIG. The first call on a device resolves the array's address
+ * (make it before any stream capture). All calls share the array: calls whose
+ * work overlaps on the GPU race. Errors: fvh_primitives_noalloc_error(). */
+int fvh_primitives_noalloc(const fvh_config* cfg, const double* u, double* w, int fv_average, void* stream);
+size_t fvh_primitives_noalloc_max_doubles(void);
+const char* fvh_primitives_noalloc_error(void);
+
 /* Copies the trouble flags of the last stage (uint8, nx*ny*nz) to the device
  * array flags. Replaces the troubled_cells array of revise_fluxes
  * (fvhoe/solver.py:691-706). */
