@@ -194,6 +194,15 @@ int configure(fvh_handle* h, const fvh_config* cfg, std::string& msg) {
   h->cfl_h = cfg->cfl * hmin;
   for (int a = 0; a < 3; ++a) h->neg_inv_h[a] = -(1.0 / cfg->h[a]);
   h->elem = cfg->precision == FVH_PREC_FP32 ? sizeof(float) : sizeof(double);
+  // kernels address arrays with 32-bit offsets: the largest (the state
+  // ghost-filled by gW + 2r cells on every active axis, all variables) must
+  // stay below 2^31 elements
+  double largest = (double)h->nv;
+  for (int a = 0; a < 3; ++a) largest *= (double)(h->n[a] + (h->active[a] ? 2 * (h->gW + 2 * h->r[a]) : 0));
+  if (largest >= 2147483648.0) {
+    msg = "grid too large: a sweep buffer would exceed 2^31 elements";
+    return FVH_ERR_CONFIG;
+  }
   int count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess) {
     cudaGetLastError();

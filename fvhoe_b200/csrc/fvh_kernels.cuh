@@ -2,8 +2,11 @@
 //
 // Every array is stored variable-major over an index box ("Region") in cell
 // coordinates: element (v, i0, i1, i2) of a box with origin lo and extents n
-// sits at ((v*n0 + i0-lo0)*n1 + i1-lo1)*n2 + i2-lo2. Axes are x, y, z in the
-// reference's order (z contiguous); an inactive axis has extent 1.
+// sits at v*vs + (i0-lo0)*n1*n2 + (i1-lo1)*n2 + (i2-lo2). Axes are x, y, z in
+// the reference's order (z contiguous); an inactive axis has extent 1.
+// Offsets are 32-bit (the configuration check keeps every array below 2^31
+// elements); a kernel forms one pointer per point and reaches its stencil
+// taps and variables by constant strides.
 //
 // The stage is a sequence of passes, each a single launch over one box:
 //   centre sweeps (the first one reads the conserved state through the
@@ -11,8 +14,8 @@
 //   transverse sweeps (the last one also reduces the CFL speed and the
 //   per-variable extrema), face reconstruction + Riemann solve, transverse
 //   sweeps of the fluxes, the candidate update, troubled-cell detection,
-//   the MUSCL fallback at troubled faces, and the flux divergence fused with
-//   the Runge-Kutta stage combination.
+//   pointwise primitives of the stage input, the MUSCL fallback at troubled
+//   faces, and the flux divergence fused with the Runge-Kutta combination.
 #pragma once
 
 #include <cstdint>
@@ -44,16 +47,80 @@ __host__ __device__ __forceinline__ int64_t region_points(const Region& r) {
   return (int64_t)r.n[0] * r.n[1] * r.n[2];
 }
 
-__device__ __forceinline__ int64_t region_index(const Region& r, int v, int i0, int i1, int i2) {
-  return (((int64_t)v * r.n[0] + (i0 - r.lo[0])) * r.n[1] + (i1 - r.lo[1])) * r.n[2] + (i2 - r.lo[2]);
+// ---------------------------------------------------------------------------
+// Division by a launch-constant divisor: q = (umulhi(n, m) + n) >> l with
+// l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1; exact for n < 2^31.
+// ---------------------------------------------------------------------------
+struct FastDiv {
+  uint32_t m;
+  uint32_t l;
+};
+
+inline FastDiv make_fastdiv(uint32_t d) {
+  FastDiv f;
+  uint32_t l = 0;
+  while ((uint64_t(1) << l) < d) ++l;
+  f.l = l;
+  f.m = (uint32_t)(((uint64_t(1) << 32) * ((uint64_t(1) << l) - d)) / d + 1);
+  return f;
 }
 
-__device__ __forceinline__ void region_point(const Region& r, int64_t idx, int& i0, int& i1, int& i2) {
-  const int64_t q = idx / r.n[2];
-  i2 = (int)(idx - q * r.n[2]) + r.lo[2];
-  const int64_t q2 = q / r.n[1];
-  i1 = (int)(q - q2 * r.n[1]) + r.lo[1];
-  i0 = (int)q2 + r.lo[0];
+__device__ __forceinline__ uint32_t fast_div(uint32_t n, const FastDiv& f) { return (__umulhi(n, f.m) + n) >> f.l; }
+
+// An index box to iterate over, with its point count and dividers.
+struct Box {
+  int lo[3];
+  int n[3];
+  FastDiv d1, d2;
+  uint32_t count;
+};
+
+inline Box make_box(const Region& r) {
+  Box b;
+  for (int a = 0; a < 3; ++a) {
+    b.lo[a] = r.lo[a];
+    b.n[a] = r.n[a];
+  }
+  b.d1 = make_fastdiv((uint32_t)r.n[1]);
+  b.d2 = make_fastdiv((uint32_t)r.n[2]);
+  b.count = (uint32_t)region_points(r);
+  return b;
+}
+
+__device__ __forceinline__ void box_point(const Box& b, uint32_t idx, int& i0, int& i1, int& i2) {
+  const uint32_t q = fast_div(idx, b.d2);
+  i2 = (int)(idx - q * (uint32_t)b.n[2]) + b.lo[2];
+  const uint32_t q2 = fast_div(q, b.d1);
+  i1 = (int)(q - q2 * (uint32_t)b.n[1]) + b.lo[1];
+  i0 = (int)q2 + b.lo[0];
+}
+
+#define FVH_FOR_POINTS(box, idx)                                                     \
+  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < (box).count; \
+       idx += gridDim.x * blockDim.x)
+
+// Strided view of a variable-major array stored over a Region.
+template <typename T>
+struct View {
+  T* p;  // element (v = 0) at the region's origin
+  int lo[3];
+  int s0, s1;  // strides of axes 0 and 1; axis 2 is contiguous
+  int vs;      // stride between variables
+  __device__ __forceinline__ int at(int i0, int i1, int i2) const {
+    return (i0 - lo[0]) * s0 + (i1 - lo[1]) * s1 + (i2 - lo[2]);
+  }
+  __device__ __forceinline__ int stride(int axis) const { return axis == 0 ? s0 : (axis == 1 ? s1 : 1); }
+};
+
+template <typename T>
+inline View<T> make_view(T* p, const Region& r) {
+  View<T> v;
+  v.p = p;
+  for (int a = 0; a < 3; ++a) v.lo[a] = r.lo[a];
+  v.s1 = r.n[2];
+  v.s0 = r.n[1] * r.n[2];
+  v.vs = r.n[0] * r.n[1] * r.n[2];
+  return v;
 }
 
 // Ghost-cell source index along one axis (fvhoe/boundary_conditions.py:60-151):
@@ -75,8 +142,12 @@ __device__ __forceinline__ int ghost_source(int i, int n, int lo_kind, int hi_ki
   return i;
 }
 
-// Reads all nv conserved variables at a (possibly ghost) cell. Reflective
-// ghosts negate the momentum normal to the wall they mirror across.
+__device__ __forceinline__ int state_stride(const Grid& g, int axis) {
+  return axis == 0 ? g.n[1] * g.n[2] : (axis == 1 ? g.n[2] : 1);
+}
+
+// Reads nv conserved variables at a (possibly ghost) cell. Reflective ghosts
+// negate the momentum normal to the wall they mirror across.
 template <typename Tc>
 __device__ __forceinline__ void load_state(const double* __restrict__ u, const Grid& g, int nv, int i0, int i1,
                                            int i2, Tc* out) {
@@ -84,19 +155,13 @@ __device__ __forceinline__ void load_state(const double* __restrict__ u, const G
   const int j0 = ghost_source(i0, g.n[0], g.bc[0][0], g.bc[0][1], f0);
   const int j1 = ghost_source(i1, g.n[1], g.bc[1][0], g.bc[1][1], f1);
   const int j2 = ghost_source(i2, g.n[2], g.bc[2][0], g.bc[2][1], f2);
-  const int64_t plane = (int64_t)g.n[0] * g.n[1] * g.n[2];
-  const int64_t base = ((int64_t)j0 * g.n[1] + j1) * g.n[2] + j2;
+  const int plane = g.n[0] * g.n[1] * g.n[2];
+  const int o = (j0 * g.n[1] + j1) * g.n[2] + j2;
   for (int v = 0; v < nv; ++v) {
-    double x = u[v * plane + base];
+    double x = u[v * plane + o];
     if ((v == 1 && f0) || (v == 2 && f1) || (v == 3 && f2)) x = -x;
     out[v] = (Tc)x;
   }
-}
-
-__device__ __forceinline__ void step_axis(int axis, int k, int& i0, int& i1, int& i2) {
-  if (axis == 0) i0 += k;
-  else if (axis == 1) i1 += k;
-  else i2 += k;
 }
 
 // Kernels take the variable count NV as a template argument: NV = 5 keeps the
@@ -143,14 +208,13 @@ struct Scalars {
 
 // Reduction request for the last transverse sweep of the primitive pass.
 struct ReduceSpec {
-  int cfl;          // reduce the CFL speed over cfl_box
+  int cfl;  // reduce the CFL speed over cfl_box
   Region cfl_box;
-  int extrema;      // reduce per-variable max/min over ext_box
+  int extrema;  // reduce per-variable max/min over ext_box
   Region ext_box;
-  double ndim;      // number of active axes, as in ndim * c
+  double ndim;  // number of active axes, as in ndim * c
 };
 
-template <typename T>
 __device__ __forceinline__ bool in_box(const Region& r, int i0, int i1, int i2) {
   return i0 >= r.lo[0] && i0 < r.lo[0] + r.n[0] && i1 >= r.lo[1] && i1 < r.lo[1] + r.n[1] && i2 >= r.lo[2] &&
          i2 < r.lo[2] + r.n[2];
@@ -171,42 +235,74 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long x)
   return x;
 }
 
+// Block-wide sum of a per-thread count with one atomic per block (blocks of
+// at most 256 threads).
+__device__ __forceinline__ void block_count_add(unsigned int count, unsigned int* dst) {
+  __shared__ unsigned int s_count[8];
+  for (int o = 16; o > 0; o >>= 1) count += __shfl_xor_sync(0xffffffffu, count, o);
+  if ((threadIdx.x & 31) == 0) s_count[threadIdx.x >> 5] = count;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int total = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) total += s_count[w];
+    if (total) atomicAdd(dst, total);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Centre-interpolation sweep (fvhoe/fv.py:106-159, 175-197). FROM_STATE reads
 // the conserved state through the ghost maps; TO_PRIMS converts the swept
 // cell-centre values to primitives (fvhoe/hydro.py:146-170).
 // ---------------------------------------------------------------------------
 template <typename Tc, typename Tin, int NV, int K, bool FROM_STATE, bool TO_PRIMS>
-__global__ void __launch_bounds__(256) k_centre_sweep(const Tin* __restrict__ in, Region rin, Tc* __restrict__ out,
-                                                      Region rout, int axis, Rule<Tc, K> rule, Grid grid,
-                                                      Phys<Tc> ph) {
+__global__ void __launch_bounds__(256)
+    k_centre_sweep(View<const Tin> in, const double* __restrict__ state, View<Tc> out, Box box, int axis,
+                   Rule<Tc, K> rule, Grid grid, Phys<Tc> ph) {
   constexpr int NVA = VarCount<NV>::kArray;
   const int nv = VarCount<NV>::get(ph);
-  const int64_t npts = region_points(rout);
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < npts;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    int i0, i1, i2;
-    region_point(rout, idx, i0, i1, i2);
+  const int plane = grid.n[0] * grid.n[1] * grid.n[2];
+  FVH_FOR_POINTS(box, idx) {
+    int i[3];
+    box_point(box, idx, i[0], i[1], i[2]);
     Tc acc[NVA];
     for (int v = 0; v < nv; ++v) acc[v] = Tc(0);
+    if constexpr (FROM_STATE) {
+      // ghost maps of the two fixed coordinates, once per point
+      bool fl[3] = {false, false, false};
+      int base = 0;
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      int j0 = i0, j1 = i1, j2 = i2;
-      step_axis(axis, rule.off + k, j0, j1, j2);
-      Tc x[NVA];
-      if constexpr (FROM_STATE) {
-        load_state<Tc>(reinterpret_cast<const double*>(in), grid, nv, j0, j1, j2, x);
-      } else {
-        for (int v = 0; v < nv; ++v) x[v] = (Tc)in[region_index(rin, v, j0, j1, j2)];
+      for (int a = 0; a < 3; ++a) {
+        if (a == axis) continue;
+        const int j = ghost_source(i[a], grid.n[a], grid.bc[a][0], grid.bc[a][1], fl[a]);
+        base += j * state_stride(grid, a);
       }
-      for (int v = 0; v < nv; ++v) acc[v] = acc[v] + rule.w[k] * x[v];
+      const int sa = state_stride(grid, axis);
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        bool fk = false;
+        const int jk = ghost_source(i[axis] + rule.off + k, grid.n[axis], grid.bc[axis][0], grid.bc[axis][1], fk);
+        const double* q = state + base + jk * sa;
+        for (int v = 0; v < nv; ++v) {
+          double x = q[v * plane];
+          const bool flip = (v >= 1 && v <= 3) && ((v - 1 == axis) ? fk : fl[v - 1]);
+          if (flip) x = -x;
+          acc[v] = acc[v] + rule.w[k] * (Tc)x;
+        }
+      }
+    } else {
+      const int sa = in.stride(axis);
+      const Tin* q = in.p + in.at(i[0], i[1], i[2]) + rule.off * sa;
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        for (int v = 0; v < nv; ++v) acc[v] = acc[v] + rule.w[k] * (Tc)q[v * in.vs + k * sa];
     }
+    Tc* o = out.p + out.at(i[0], i[1], i[2]);
     if constexpr (TO_PRIMS) {
       Tc w[NVA];
       to_primitives(ph, nv, acc, w);
-      for (int v = 0; v < nv; ++v) out[region_index(rout, v, i0, i1, i2)] = w[v];
+      for (int v = 0; v < nv; ++v) o[v * out.vs] = w[v];
     } else {
-      for (int v = 0; v < nv; ++v) out[region_index(rout, v, i0, i1, i2)] = acc[v];
+      for (int v = 0; v < nv; ++v) o[v * out.vs] = acc[v];
     }
   }
 }
@@ -217,12 +313,11 @@ __global__ void __launch_bounds__(256) k_centre_sweep(const Tin* __restrict__ in
 // used by global NAD (fvhoe/slope_limiting.py:165-170, 184-185).
 // ---------------------------------------------------------------------------
 template <typename Tc, int NV, int K, bool REDUCE>
-__global__ void __launch_bounds__(256) k_transverse_sweep(const Tc* __restrict__ in, Region rin, Tc* __restrict__ out,
-                                                          Region rout, int axis, Rule<Tc, K> rule, Phys<Tc> ph,
-                                                          ReduceSpec rs, Scalars* __restrict__ sc) {
+__global__ void __launch_bounds__(256)
+    k_transverse_sweep(View<const Tc> in, View<Tc> out, Box box, int axis, Rule<Tc, K> rule, Phys<Tc> ph,
+                       ReduceSpec rs, Scalars* __restrict__ sc) {
   constexpr int NVA = VarCount<NV>::kArray;
   const int nv = VarCount<NV>::get(ph);
-  const int64_t npts = region_points(rout);
   unsigned long long cfl_key = 0ull;
   unsigned long long kmax[5], kmin[5];
   if constexpr (REDUCE) {
@@ -231,25 +326,24 @@ __global__ void __launch_bounds__(256) k_transverse_sweep(const Tc* __restrict__
       kmin[v] = ~0ull;
     }
   }
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < npts;
-       idx += (int64_t)gridDim.x * blockDim.x) {
+  const int sa = in.stride(axis);
+  FVH_FOR_POINTS(box, idx) {
     int i0, i1, i2;
-    region_point(rout, idx, i0, i1, i2);
+    box_point(box, idx, i0, i1, i2);
     Tc acc[NVA];
     for (int v = 0; v < nv; ++v) acc[v] = Tc(0);
+    const Tc* q = in.p + in.at(i0, i1, i2) + rule.off * sa;
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      int j0 = i0, j1 = i1, j2 = i2;
-      step_axis(axis, rule.off + k, j0, j1, j2);
-      for (int v = 0; v < nv; ++v) acc[v] = acc[v] + rule.w[k] * in[region_index(rin, v, j0, j1, j2)];
-    }
-    for (int v = 0; v < nv; ++v) out[region_index(rout, v, i0, i1, i2)] = acc[v];
+    for (int k = 0; k < K; ++k)
+      for (int v = 0; v < nv; ++v) acc[v] = acc[v] + rule.w[k] * q[v * in.vs + k * sa];
+    Tc* o = out.p + out.at(i0, i1, i2);
+    for (int v = 0; v < nv; ++v) o[v * out.vs] = acc[v];
     if constexpr (REDUCE) {
-      if (rs.cfl && in_box<Tc>(rs.cfl_box, i0, i1, i2)) {
+      if (rs.cfl && in_box(rs.cfl_box, i0, i1, i2)) {
         const unsigned long long k = order_key((double)cfl_speed(ph, acc, (Tc)rs.ndim));
         cfl_key = k > cfl_key ? k : cfl_key;
       }
-      if (rs.extrema && in_box<Tc>(rs.ext_box, i0, i1, i2)) {
+      if (rs.extrema && in_box(rs.ext_box, i0, i1, i2)) {
         for (int v = 0; v < 5; ++v) {
           const unsigned long long k = order_key((double)acc[v]);
           kmax[v] = k > kmax[v] ? k : kmax[v];
@@ -292,36 +386,24 @@ __global__ void __launch_bounds__(256) k_transverse_sweep(const Tc* __restrict__
   }
 }
 
-// Block-wide sum of a per-thread count with one atomic per block (blocks of
-// at most 256 threads).
-__device__ __forceinline__ void block_count_add(unsigned int count, unsigned int* dst) {
-  __shared__ unsigned int s_count[8];
-  for (int o = 16; o > 0; o >>= 1) count += __shfl_xor_sync(0xffffffffu, count, o);
-  if ((threadIdx.x & 31) == 0) s_count[threadIdx.x >> 5] = count;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned int total = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) total += s_count[w];
-    if (total) atomicAdd(dst, total);
-  }
-}
-
 // ---------------------------------------------------------------------------
 // Face reconstruction along d and the Riemann solve (fvhoe/solver.py:522-607):
 // face j lies between cells j-1 and j; the left state is cell j-1's right-face
 // value, the right state is cell j's left-face value.
 // ---------------------------------------------------------------------------
 template <typename Tc, int NV, int K>
-__global__ void __launch_bounds__(256) k_face_riemann(const Tc* __restrict__ in, Region rin, Tc* __restrict__ out,
-                                                      Region rout, int d, Rule<Tc, K> left_rule,
-                                                      Rule<Tc, K> right_rule, Phys<Tc> ph) {
+__global__ void __launch_bounds__(256)
+    k_face_riemann(View<const Tc> in, View<Tc> out, Box box, int d, Rule<Tc, K> left_rule, Rule<Tc, K> right_rule,
+                   Phys<Tc> ph) {
   constexpr int NVA = VarCount<NV>::kArray;
   const int nv = VarCount<NV>::get(ph);
-  const int64_t npts = region_points(rout);
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < npts;
-       idx += (int64_t)gridDim.x * blockDim.x) {
+  const int sd = in.stride(d);
+  FVH_FOR_POINTS(box, idx) {
     int i0, i1, i2;
-    region_point(rout, idx, i0, i1, i2);
+    box_point(box, idx, i0, i1, i2);
+    const Tc* q = in.p + in.at(i0, i1, i2);
+    const Tc* qa = q + (right_rule.off - 1) * sd;  // cell j-1, right-face rule
+    const Tc* qb = q + left_rule.off * sd;         // cell j, left-face rule
     Tc wl[NVA], wr[NVA];
     for (int v = 0; v < nv; ++v) {
       wl[v] = Tc(0);
@@ -329,18 +411,15 @@ __global__ void __launch_bounds__(256) k_face_riemann(const Tc* __restrict__ in,
     }
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      int a0 = i0, a1 = i1, a2 = i2;
-      step_axis(d, right_rule.off + k - 1, a0, a1, a2);  // cell j-1, right-face rule
-      int b0 = i0, b1 = i1, b2 = i2;
-      step_axis(d, left_rule.off + k, b0, b1, b2);  // cell j, left-face rule
       for (int v = 0; v < nv; ++v) {
-        wl[v] = wl[v] + right_rule.w[k] * in[region_index(rin, v, a0, a1, a2)];
-        wr[v] = wr[v] + left_rule.w[k] * in[region_index(rin, v, b0, b1, b2)];
+        wl[v] = wl[v] + right_rule.w[k] * qa[v * in.vs + k * sd];
+        wr[v] = wr[v] + left_rule.w[k] * qb[v * in.vs + k * sd];
       }
     }
     Tc f[NVA];
     riemann_flux<NVA>(ph, nv, wl, wr, d, f);
-    for (int v = 0; v < nv; ++v) out[region_index(rout, v, i0, i1, i2)] = f[v];
+    Tc* o = out.p + out.at(i0, i1, i2);
+    for (int v = 0; v < nv; ++v) o[v * out.vs] = f[v];
   }
 }
 
@@ -348,53 +427,46 @@ __global__ void __launch_bounds__(256) k_face_riemann(const Tc* __restrict__ in,
 // Flux divergence, fvhoe/solver.py:734-751:
 //   dudt = 0.0 + -(1/hx)(F[i+1]-F[i]) + -(1/hy)(G[j+1]-G[j]) + -(1/hz)(H[k+1]-H[k])
 // ---------------------------------------------------------------------------
+template <typename Tc>
 struct FluxSet {
-  const void* f[3];  // per-axis face fluxes (nullptr for inactive axes)
-  Region r[3];
+  View<const Tc> f[3];
+  int has[3];
   double neg_inv_h[3];  // -(1/h_d), rounded on the host as Python does
 };
 
 template <typename Tc>
-__device__ __forceinline__ void divergence(const FluxSet& fs, int nv, int i0, int i1, int i2, Tc* dudt) {
+__device__ __forceinline__ void divergence(const FluxSet<Tc>& fs, int nv, int i0, int i1, int i2, Tc* dudt) {
   for (int v = 0; v < nv; ++v) dudt[v] = Tc(0);
+#pragma unroll
   for (int d = 0; d < 3; ++d) {
-    if (!fs.f[d]) continue;
-    const Tc* F = reinterpret_cast<const Tc*>(fs.f[d]);
-    int a0 = i0, a1 = i1, a2 = i2;
-    step_axis(d, 1, a0, a1, a2);
+    if (!fs.has[d]) continue;
+    const View<const Tc>& F = fs.f[d];
+    const Tc* q = F.p + F.at(i0, i1, i2);
+    const int sd = F.stride(d);
     const Tc c = (Tc)fs.neg_inv_h[d];
-    for (int v = 0; v < nv; ++v) {
-      const Tc hi = (Tc)F[region_index(fs.r[d], v, a0, a1, a2)];
-      const Tc lo = (Tc)F[region_index(fs.r[d], v, i0, i1, i2)];
-      dudt[v] = dudt[v] + c * (hi - lo);
-    }
+    for (int v = 0; v < nv; ++v) dudt[v] = dudt[v] + c * (q[v * F.vs + sd] - q[v * F.vs]);
   }
 }
 
-// Candidate state u* = u + dt L(F) (fvhoe/solver.py:677-678).
+// Candidate state u* = u + dt L(F) (fvhoe/solver.py:677-678), kept in float64.
 template <typename Tc, int NV>
-__global__ void __launch_bounds__(256) k_candidate(const double* __restrict__ u, Region rint, FluxSet fs,
-                                                   double* __restrict__ ustar, Phys<Tc> ph,
-                                                   const Scalars* __restrict__ sc) {
+__global__ void __launch_bounds__(256) k_candidate(const double* __restrict__ u, View<double> ustar, Box box,
+                                                   FluxSet<Tc> fs, Phys<Tc> ph, const Scalars* __restrict__ sc) {
   constexpr int NVA = VarCount<NV>::kArray;
   const int nv = VarCount<NV>::get(ph);
-  const int64_t npts = region_points(rint);
   const double dt = sc->dt_stage;
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < npts;
-       idx += (int64_t)gridDim.x * blockDim.x) {
+  FVH_FOR_POINTS(box, idx) {
     int i0, i1, i2;
-    region_point(rint, idx, i0, i1, i2);
+    box_point(box, idx, i0, i1, i2);
     Tc dudt[NVA];
     divergence<Tc>(fs, nv, i0, i1, i2, dudt);
-    for (int v = 0; v < nv; ++v) {
-      const int64_t o = region_index(rint, v, i0, i1, i2);
-      ustar[o] = u[o] + dt * (double)dudt[v];
-    }
+    const int o = ustar.at(i0, i1, i2);
+    for (int v = 0; v < nv; ++v) ustar.p[v * ustar.vs + o] = u[v * ustar.vs + o] + dt * (double)dudt[v];
   }
 }
 
 // ---------------------------------------------------------------------------
-// Troubled-cell detection (fvhoe/slope_limiting.py:87-244).
+// Troubled-cell detection (fvhoe/slope_limiting.py:87-244), for NDIM active axes.
 // ---------------------------------------------------------------------------
 struct DetectSpec {
   int nad_global;    // 1: range from the global extrema, 0: local box range
@@ -406,92 +478,131 @@ struct DetectSpec {
   int pad_var;  // -1 when PAD is off; otherwise the primitive index of the last PAD key
   double pad_lo, pad_hi;
   int force_trouble;
-  int active[3];
+  int axes[3];   // the active axes, ascending
   int log_mode;  // 0: no logging, 1: overwrite the running sums, 2: add to them
 };
 
-template <typename Tc>
-__global__ void __launch_bounds__(256) k_detect(const Tc* __restrict__ w, Region rw, const Tc* __restrict__ ws,
-                                                Region rws, Region rint, DetectSpec ds, Scalars* __restrict__ sc,
-                                                uint8_t* __restrict__ trouble, double* __restrict__ log_trouble,
-                                                double* __restrict__ log_nad, double* __restrict__ log_pad) {
-  const int64_t npts = region_points(rint);
+// Whether the smooth-extrema detector's alpha along one line is below 1
+// (fvhoe/smooth_extrema_detection.py:8-50). a[0..6] are the values at
+// offsets -3..+3. The reference takes alpha = min over the cell and its two
+// neighbours of min(alpha_L, alpha_R), with alpha_L clamped to 1 and alpha_R
+// set to 1 where |dv| <= eps; alpha < 1 exactly when some alpha_L or alpha_R
+// of the three positions is, so the scan stops at the first one found. Each
+// alpha is the same quotient the reference forms.
+template <typename T>
+__device__ __forceinline__ bool sed_line_below_one(const T* a, T eps) {
+  T du[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) du[k] = T(0.5) * (a[k + 2] - a[k]);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const T d2u = T(0.5) * (du[k + 2] - du[k]);
+    T dv = T(0.5) * d2u;
+    const bool small = fabs(dv) <= eps;
+    if (small) dv = dv >= T(0) ? eps : -eps;
+    const T vl = du[k] - du[k + 1];
+    const T xl = dv < T(0) ? (vl > T(0) ? vl : T(0)) : (vl < T(0) ? vl : T(0));
+    // alpha_L = -x_L / dv; a zero numerator gives a zero alpha without dividing
+    if (xl == T(0) || -xl / dv < T(1)) return true;
+    if (fabs(dv) > eps) {
+      const T vr = du[k + 2] - du[k + 1];
+      const T xr = dv > T(0) ? (vr > T(0) ? vr : T(0)) : (vr < T(0) ? vr : T(0));
+      if (xr == T(0) || xr / dv < T(1)) return true;
+    }
+  }
+  return false;
+}
+
+template <typename Tc, int NDIM>
+__global__ void __launch_bounds__(256)
+    k_detect(View<const Tc> w, View<const Tc> ws, Box box, DetectSpec ds, Scalars* __restrict__ sc,
+             View<uint8_t> trouble, double* __restrict__ log_trouble, double* __restrict__ log_nad,
+             double* __restrict__ log_pad) {
+  int sw[3] = {0, 0, 0}, sws[3] = {0, 0, 0};
+#pragma unroll
+  for (int k = 0; k < NDIM; ++k) {
+    sw[k] = w.stride(ds.axes[k]);
+    sws[k] = ws.stride(ds.axes[k]);
+  }
+  // NAD bounds that do not depend on the cell
+  Tc grange[5], glower[5], gupper[5];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) {
+    const double vmax = key_value(sc->vmax_key[v]);
+    const double vmin = key_value(sc->vmin_key[v]);
+    grange[v] = (Tc)(vmax - vmin);
+    glower[v] = (Tc)((1.0 - ds.nad_eps) * vmin);
+    gupper[v] = (Tc)((1.0 + ds.nad_eps) * vmax);
+  }
+  const Tc neg_eps = (Tc)(-ds.nad_eps);
+  const Tc lo_fac = (Tc)(1.0 - ds.nad_eps), hi_fac = (Tc)(1.0 + ds.nad_eps);
+  const Tc sed_eps = (Tc)ds.sed_eps;
   unsigned int count = 0;
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < npts;
-       idx += (int64_t)gridDim.x * blockDim.x) {
+  FVH_FOR_POINTS(box, idx) {
     int i0, i1, i2;
-    region_point(rint, idx, i0, i1, i2);
-    const int r0 = ds.active[0], r1 = ds.active[1], r2 = ds.active[2];
+    box_point(box, idx, i0, i1, i2);
+    const int ow = w.at(i0, i1, i2);
+    const int ows = ws.at(i0, i1, i2);
     bool nad_any = false;
     Tc ind_min = Tc(0);
     Tc pad_ind = Tc(0);
+#pragma unroll
     for (int v = 0; v < 5; ++v) {
       // 3^d box extrema of w (fvhoe/slope_limiting.py:145-162)
-      Tc big = w[region_index(rw, v, i0, i1, i2)], small = big;
-      for (int a = -r0; a <= r0; ++a)
-        for (int b = -r1; b <= r1; ++b)
-          for (int c = -r2; c <= r2; ++c) {
-            const Tc x = w[region_index(rw, v, i0 + a, i1 + b, i2 + c)];
-            big = np_maximum(big, x);
-            small = np_minimum(small, x);
+      const Tc* pw = w.p + v * w.vs + ow;
+      Tc big = pw[0], small = big;
+#pragma unroll
+      for (int a = -1; a <= 1; ++a)
+#pragma unroll
+        for (int b = (NDIM > 1 ? -1 : 0); b <= (NDIM > 1 ? 1 : 0); ++b)
+#pragma unroll
+          for (int c = (NDIM > 2 ? -1 : 0); c <= (NDIM > 2 ? 1 : 0); ++c) {
+            const Tc x = pw[a * sw[0] + b * sw[1] + c * sw[2]];
+            big = fmax(big, x);
+            small = fmin(small, x);
           }
-      const Tc xs = ws[region_index(rws, v, i0, i1, i2)];
+      const Tc* pws = ws.p + v * ws.vs + ows;
+      const Tc xs = pws[0];
       Tc ind;
       bool tv;
       if (ds.nad_relative) {
-        Tc range;
-        if (ds.nad_global) {
-          range = (Tc)(key_value(sc->vmax_key[v]) - key_value(sc->vmin_key[v]));
-        } else {
-          range = big - small;
-        }
+        const Tc range = ds.nad_global ? grange[v] : big - small;
         ind = xs - small;
-        ind = np_minimum(ind, big - xs);
-        tv = ind < (Tc)(-ds.nad_eps) * range;
+        ind = fmin(ind, big - xs);
+        tv = ind < neg_eps * range;
       } else {
-        Tc lower, upper;
-        if (ds.nad_global) {
-          lower = (Tc)((1.0 - ds.nad_eps) * key_value(sc->vmin_key[v]));
-          upper = (Tc)((1.0 + ds.nad_eps) * key_value(sc->vmax_key[v]));
-        } else {
-          lower = (Tc)(1.0 - ds.nad_eps) * small;
-          upper = (Tc)(1.0 + ds.nad_eps) * big;
-        }
-        ind = np_minimum(xs - lower, upper - xs);
+        const Tc lower = ds.nad_global ? glower[v] : lo_fac * small;
+        const Tc upper = ds.nad_global ? gupper[v] : hi_fac * big;
+        ind = fmin(xs - lower, upper - xs);
         tv = ind < Tc(0);
       }
       if (tv && ds.sed) {
-        // smooth-extrema detector on w* (fvhoe/smooth_extrema_detection.py:8-95)
-        Tc alpha = Tc(0);
-        bool first = true;
-        for (int a = 0; a < 3; ++a) {
-          if (!ds.active[a]) continue;
+        // smooth-extrema detector on w* (fvhoe/smooth_extrema_detection.py:8-95):
+        // the flag survives only where alpha, the minimum over the axes, is below 1
+        bool below = false;
+#pragma unroll
+        for (int k = 0; k < NDIM; ++k) {
+          if (below) break;
           Tc line[7];
 #pragma unroll
-          for (int k = 0; k < 7; ++k) {
-            int j0 = i0, j1 = i1, j2 = i2;
-            step_axis(a, k - 3, j0, j1, j2);
-            line[k] = ws[region_index(rws, v, j0, j1, j2)];
-          }
-          const Tc al = sed_alpha_line(line, (Tc)ds.sed_eps);
-          alpha = first ? al : np_minimum(alpha, al);
-          first = false;
+          for (int m = 0; m < 7; ++m) line[m] = pws[(m - 3) * sws[k]];
+          below = sed_line_below_one(line, sed_eps);
         }
-        tv = alpha < Tc(1);
+        tv = below;
       }
       if (!((ds.nad_var_mask >> v) & 1)) tv = false;
       nad_any = nad_any || tv;
-      ind_min = (v == 0) ? ind : np_minimum(ind_min, ind);
+      ind_min = (v == 0) ? ind : fmin(ind_min, ind);
       if (v == ds.pad_var) {
         pad_ind = xs - (Tc)ds.pad_lo;
-        pad_ind = np_minimum(pad_ind, (Tc)ds.pad_hi - xs);
+        pad_ind = fmin(pad_ind, (Tc)ds.pad_hi - xs);
       }
     }
     const bool pad_trouble = pad_ind < Tc(0);
     bool t = pad_trouble || nad_any;
     if (ds.force_trouble) t = true;
-    const int64_t o = region_index(rint, 0, i0, i1, i2);
-    trouble[o] = t ? 1 : 0;
+    const int o = trouble.at(i0, i1, i2);
+    trouble.p[o] = t ? 1 : 0;
     count += t ? 1u : 0u;
     if (ds.log_mode) {
       const double lt = t ? 1.0 : 0.0;
@@ -512,76 +623,86 @@ __global__ void __launch_bounds__(256) k_detect(const Tc* __restrict__ w, Region
 }
 
 // ---------------------------------------------------------------------------
+// Pointwise primitives of the stage input over the interior and 2 ghost
+// cells: the fallback scheme's FV primitives, because its p = 1 centre and
+// transverse rules are the identity (fvhoe/solver.py:712-717, 753-792).
+// ---------------------------------------------------------------------------
+template <typename Tc, int NV>
+__global__ void __launch_bounds__(256) k_pointwise_primitives(const double* __restrict__ u, Grid grid, View<Tc> w1,
+                                                              Box box, Phys<Tc> ph) {
+  constexpr int NVA = VarCount<NV>::kArray;
+  const int nv = VarCount<NV>::get(ph);
+  FVH_FOR_POINTS(box, idx) {
+    int i0, i1, i2;
+    box_point(box, idx, i0, i1, i2);
+    Tc uc[NVA], w[NVA];
+    load_state<Tc>(u, grid, nv, i0, i1, i2, uc);
+    to_primitives(ph, nv, uc, w);
+    Tc* o = w1.p + w1.at(i0, i1, i2);
+    for (int v = 0; v < nv; ++v) o[v * w1.vs] = w[v];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // MUSCL fallback at troubled faces and the flux blend
 // (fvhoe/solver.py:710-731, fvhoe/slope_limiting.py:24-84, 247-384).
 // theta of face j = max(trouble[j-1], trouble[j]) with missing neighbours 0,
 // or the convex weights when theta_in is given.
 // ---------------------------------------------------------------------------
 struct FallbackSpec {
-  int d;             // face-normal axis
-  int muscl;         // 1: slope-limited p=1 reconstruction along d, 0: first order
-  int limiter;       // Limiter enum
-  Region rflux;      // region of F_d
-  Region rint;       // interior region
+  int d;        // face-normal axis
+  int nd;       // interior cells along d
+  int muscl;    // 1: slope-limited p=1 reconstruction along d, 0: first order
+  int limiter;  // Limiter enum
 };
 
 template <typename Tc, int NV>
-__global__ void __launch_bounds__(256) k_fallback(const double* __restrict__ u, Grid grid, Tc* __restrict__ F,
-                                                  const uint8_t* __restrict__ trouble, const float* __restrict__ theta_in,
-                                                  FallbackSpec fb, Phys<Tc> ph) {
+__global__ void __launch_bounds__(256)
+    k_fallback(View<const Tc> w1, View<Tc> F, Box box, View<const uint8_t> trouble, const float* __restrict__ theta_in,
+               FallbackSpec fb, Phys<Tc> ph) {
   constexpr int NVA = VarCount<NV>::kArray;
   const int nv = VarCount<NV>::get(ph);
-  const int64_t npts = region_points(fb.rflux);
   const int d = fb.d;
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < npts;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    int i0, i1, i2;
-    region_point(fb.rflux, idx, i0, i1, i2);
+  const int st = trouble.stride(d);
+  const int sw = w1.stride(d);
+  FVH_FOR_POINTS(box, idx) {
+    int i[3];
+    box_point(box, idx, i[0], i[1], i[2]);
     Tc theta;
     if (theta_in) {
       theta = (Tc)theta_in[idx];
     } else {
-      const int j = d == 0 ? i0 : (d == 1 ? i1 : i2);
-      const int nd = grid.n[d];
-      int a0 = i0, a1 = i1, a2 = i2;
-      step_axis(d, -1, a0, a1, a2);
-      const uint8_t tl = j >= 1 ? trouble[region_index(fb.rint, 0, a0, a1, a2)] : 0;
-      const uint8_t tr = j < nd ? trouble[region_index(fb.rint, 0, i0, i1, i2)] : 0;
+      const int j = i[d];
+      const int ot = trouble.at(i[0], i[1], i[2]);
+      const uint8_t tl = j >= 1 ? trouble.p[ot - st] : 0;
+      const uint8_t tr = j < fb.nd ? trouble.p[ot] : 0;
       theta = (tl || tr) ? Tc(1) : Tc(0);
     }
     if (!(theta > Tc(0))) continue;
-    // primitives at cells j-2 .. j+1 along d (p=1 centre/transverse rules are identities)
-    Tc w[4][NVA];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      int a0 = i0, a1 = i1, a2 = i2;
-      step_axis(d, c - 2, a0, a1, a2);
-      Tc uc[NVA];
-      load_state<Tc>(u, grid, nv, a0, a1, a2, uc);
-      to_primitives(ph, nv, uc, w[c]);
-    }
+    // primitives at cells j-2 .. j+1 along d
+    const Tc* q = w1.p + w1.at(i[0], i[1], i[2]) - 2 * sw;
     Tc wl[NVA], wr[NVA];
     for (int v = 0; v < nv; ++v) {
+      const Tc* qv = q + v * w1.vs;
+      const Tc a0 = qv[0], a1 = qv[sw], a2 = qv[2 * sw], a3 = qv[3 * sw];
       if (fb.muscl && fb.limiter == LIMITER_NONE) {
         // unlimited p=1 face rules [1/4, 1, -1/4] and its mirror (fvhoe/stencils.py:44-46)
-        wl[v] = ((Tc(0) + Tc(-0.25) * w[0][v]) + Tc(1) * w[1][v]) + Tc(0.25) * w[2][v];
-        wr[v] = ((Tc(0) + Tc(0.25) * w[1][v]) + Tc(1) * w[2][v]) + Tc(-0.25) * w[3][v];
+        wl[v] = ((Tc(0) + Tc(-0.25) * a0) + Tc(1) * a1) + Tc(0.25) * a2;
+        wr[v] = ((Tc(0) + Tc(0.25) * a1) + Tc(1) * a2) + Tc(-0.25) * a3;
       } else if (fb.muscl) {
-        const Tc sl = limited_slope(w[1][v] - w[0][v], w[2][v] - w[1][v], fb.limiter);
-        const Tc sr = limited_slope(w[2][v] - w[1][v], w[3][v] - w[2][v], fb.limiter);
-        wl[v] = w[1][v] + Tc(0.5) * sl;
-        wr[v] = w[2][v] - Tc(0.5) * sr;
+        const Tc sl = limited_slope(a1 - a0, a2 - a1, fb.limiter);
+        const Tc sr = limited_slope(a2 - a1, a3 - a2, fb.limiter);
+        wl[v] = a1 + Tc(0.5) * sl;
+        wr[v] = a2 - Tc(0.5) * sr;
       } else {
-        wl[v] = w[1][v];
-        wr[v] = w[2][v];
+        wl[v] = a1;
+        wr[v] = a2;
       }
     }
     Tc flo[NVA];
     riemann_flux<NVA>(ph, nv, wl, wr, d, flo);
-    for (int v = 0; v < nv; ++v) {
-      const int64_t o = region_index(fb.rflux, v, i0, i1, i2);
-      F[o] = (Tc(1) - theta) * F[o] + theta * flo[v];
-    }
+    Tc* o = F.p + F.at(i[0], i[1], i[2]);
+    for (int v = 0; v < nv; ++v) o[v * F.vs] = (Tc(1) - theta) * o[v * F.vs] + theta * flo[v];
   }
 }
 
@@ -610,21 +731,20 @@ struct StageSpec {
 };
 
 template <typename Tc, int NV>
-__global__ void __launch_bounds__(256) k_final(Region rint, FluxSet fs, Phys<Tc> ph, StageSpec st,
-                                               Scalars* __restrict__ sc) {
+__global__ void __launch_bounds__(256) k_final(Box box, View<double> state, FluxSet<Tc> fs, Phys<Tc> ph,
+                                               StageSpec st, Scalars* __restrict__ sc) {
   constexpr int NVA = VarCount<NV>::kArray;
   const int nv = VarCount<NV>::get(ph);
-  const int64_t npts = region_points(rint);
   const double dt = sc->dt_step;
   unsigned int bad = 0;
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < npts;
-       idx += (int64_t)gridDim.x * blockDim.x) {
+  FVH_FOR_POINTS(box, idx) {
     int i0, i1, i2;
-    region_point(rint, idx, i0, i1, i2);
+    box_point(box, idx, i0, i1, i2);
     Tc dudt_c[NVA];
     divergence<Tc>(fs, nv, i0, i1, i2, dudt_c);
+    const int base = state.at(i0, i1, i2);
     for (int v = 0; v < nv; ++v) {
-      const int64_t o = region_index(rint, v, i0, i1, i2);
+      const int o = base + v * state.vs;
       const double k = (double)dudt_c[v];
       double res = 0.0;
       switch (st.integrator) {

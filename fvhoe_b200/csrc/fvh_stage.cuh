@@ -167,23 +167,27 @@ template <typename Tc, int NV, int K>
 void launch_centre_k(bool from_state, bool to_prims, const void* in, Region rin, Tc* out, Region rout, int axis,
                      const HostRule& hr, const Grid& g, const Phys<Tc>& ph, cudaStream_t s) {
   const Rule<Tc, K> rule = device_rule<Tc, K>(hr);
+  const Box box = make_box(rout);
+  const View<Tc> vo = make_view(out, rout);
   const unsigned nb = blocks_for(region_points(rout));
   LaunchScope scope(KK_CENTRE,
                     region_bytes(rout, ph.nv, from_state ? sizeof(double) : sizeof(Tc), axis, K - 1) +
                         region_bytes(rout, ph.nv, sizeof(Tc)),
                     s);
   if (from_state) {
+    const View<const double> none = make_view((const double*)nullptr, rout);
     if (to_prims)
       k_centre_sweep<Tc, double, NV, K, true, true>
-          <<<nb, 256, 0, s>>>((const double*)in, rin, out, rout, axis, rule, g, ph);
+          <<<nb, 256, 0, s>>>(none, (const double*)in, vo, box, axis, rule, g, ph);
     else
       k_centre_sweep<Tc, double, NV, K, true, false>
-          <<<nb, 256, 0, s>>>((const double*)in, rin, out, rout, axis, rule, g, ph);
+          <<<nb, 256, 0, s>>>(none, (const double*)in, vo, box, axis, rule, g, ph);
   } else {
+    const View<const Tc> vi = make_view((const Tc*)in, rin);
     if (to_prims)
-      k_centre_sweep<Tc, Tc, NV, K, false, true><<<nb, 256, 0, s>>>((const Tc*)in, rin, out, rout, axis, rule, g, ph);
+      k_centre_sweep<Tc, Tc, NV, K, false, true><<<nb, 256, 0, s>>>(vi, nullptr, vo, box, axis, rule, g, ph);
     else
-      k_centre_sweep<Tc, Tc, NV, K, false, false><<<nb, 256, 0, s>>>((const Tc*)in, rin, out, rout, axis, rule, g, ph);
+      k_centre_sweep<Tc, Tc, NV, K, false, false><<<nb, 256, 0, s>>>(vi, nullptr, vo, box, axis, rule, g, ph);
   }
 }
 
@@ -203,14 +207,17 @@ template <typename Tc, int NV, int K>
 void launch_transverse_k(bool reduce, const Tc* in, Region rin, Tc* out, Region rout, int axis, const HostRule& hr,
                          const Phys<Tc>& ph, const ReduceSpec& rs, Scalars* sc, cudaStream_t s) {
   const Rule<Tc, K> rule = device_rule<Tc, K>(hr);
+  const Box box = make_box(rout);
+  const View<const Tc> vi = make_view(in, rin);
+  const View<Tc> vo = make_view(out, rout);
   // reducing sweeps use a bounded, grid-stride grid so each block folds many points
   const unsigned nb = reduce ? std::min(blocks_for(region_points(rout)), 148u * 8u) : blocks_for(region_points(rout));
   LaunchScope scope(KK_TRANSVERSE,
                     region_bytes(rout, ph.nv, sizeof(Tc), axis, K - 1) + region_bytes(rout, ph.nv, sizeof(Tc)), s);
   if (reduce)
-    k_transverse_sweep<Tc, NV, K, true><<<nb, 256, 0, s>>>(in, rin, out, rout, axis, rule, ph, rs, sc);
+    k_transverse_sweep<Tc, NV, K, true><<<nb, 256, 0, s>>>(vi, vo, box, axis, rule, ph, rs, sc);
   else
-    k_transverse_sweep<Tc, NV, K, false><<<nb, 256, 0, s>>>(in, rin, out, rout, axis, rule, ph, rs, sc);
+    k_transverse_sweep<Tc, NV, K, false><<<nb, 256, 0, s>>>(vi, vo, box, axis, rule, ph, rs, sc);
 }
 
 template <typename Tc, int NV>
@@ -230,7 +237,7 @@ void launch_face_k(const Tc* in, Region rin, Tc* out, Region rout, int d, const 
                    const Phys<Tc>& ph, cudaStream_t s) {
   LaunchScope scope(KK_FACE, region_bytes(rout, ph.nv, sizeof(Tc), d, K) + region_bytes(rout, ph.nv, sizeof(Tc)), s);
   k_face_riemann<Tc, NV, K><<<blocks_for(region_points(rout)), 256, 0, s>>>(
-      in, rin, out, rout, d, device_rule<Tc, K>(l), device_rule<Tc, K>(r), ph);
+      make_view(in, rin), make_view(out, rout), make_box(rout), d, device_rule<Tc, K>(l), device_rule<Tc, K>(r), ph);
 }
 
 template <typename Tc, int NV>
@@ -379,13 +386,14 @@ int flux_pass(fvh_handle* h, const Tc* W, Region rW, int d, Tc* Fd, cudaStream_t
 // padding writes an empty slice unless all three axes are active, so the
 // padding stays zero in 1D and 2D.)
 // ---------------------------------------------------------------------------
-__global__ void k_convex_init(const uint8_t* __restrict__ trouble, Region rint, Region rpad, float* __restrict__ th);
-__global__ void k_convex_step(const float* __restrict__ src, const float* __restrict__ prev, float* __restrict__ out,
-                              Region rpad, int s0, int s1, int s2, float coef, int src_is_theta);
-__global__ void k_convex_faces(const float* __restrict__ th, Region rpad, float* __restrict__ theta, Region rflux,
-                               int d);
-
 int convex_weights(fvh_handle* h, cudaStream_t s);
+
+template <int NDIM, typename Tc>
+void launch_detect(const fvh_handle* h, const View<const Tc>& w, const View<const Tc>& ws, const Box& box,
+                   const DetectSpec& ds, const View<uint8_t>& tr, cudaStream_t s) {
+  k_detect<Tc, NDIM><<<blocks_for(box.count), 256, 0, s>>>(w, ws, box, ds, h->sc, tr, h->logs[0], h->logs[1],
+                                                           h->logs[2]);
+}
 
 // ---------------------------------------------------------------------------
 // one stage
@@ -416,15 +424,16 @@ int run_stage_t(fvh_handle* h, const StageCall& c, cudaStream_t s) {
                                   c.t, c.target);
   }
   // 3. high-order fluxes
-  FluxSet fs{};
+  FluxSet<Tc> fs{};
   for (int d = 0; d < 3; ++d) {
     if (!h->active[d]) continue;
     if ((st = flux_pass<Tc, NV>(h, (const Tc*)h->W, rW, d, (Tc*)h->F[d], s))) return st;
-    fs.f[d] = h->F[d];
-    fs.r[d] = face_region(h, d);
+    fs.f[d] = make_view((const Tc*)h->F[d], face_region(h, d));
+    fs.has[d] = 1;
     fs.neg_inv_h[d] = h->neg_inv_h[d];
   }
   const Region rint = interior_region(h);
+  const Box bint = make_box(rint);
   double flux_bytes = 0.0;
   for (int d = 0; d < 3; ++d)
     if (h->active[d]) flux_bytes += region_bytes(face_region(h, d), h->nv, sizeof(Tc));
@@ -433,7 +442,8 @@ int run_stage_t(fvh_handle* h, const StageCall& c, cudaStream_t s) {
   if (apost) {
     {
       LaunchScope scope(KK_CANDIDATE, 2 * state_bytes + flux_bytes, s);
-      k_candidate<Tc, NV><<<blocks_for(region_points(rint)), 256, 0, s>>>(c.stage_in, rint, fs, h->Us, ph, h->sc);
+      k_candidate<Tc, NV><<<blocks_for(bint.count), 256, 0, s>>>(c.stage_in, make_view(h->Us, rint), bint, fs, ph,
+                                                                 h->sc);
     }
     if ((st = set_cuda_error(h, "candidate"))) return st;
     ReduceSpec none{};
@@ -449,7 +459,9 @@ int run_stage_t(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     ds.pad_lo = cfg.pad_lo;
     ds.pad_hi = cfg.pad_hi;
     ds.force_trouble = cfg.force_trouble;
-    for (int a = 0; a < 3; ++a) ds.active[a] = h->active[a] ? 1 : 0;
+    int na = 0;
+    for (int a = 0; a < 3; ++a)
+      if (h->active[a]) ds.axes[na++] = a;
     ds.log_mode = cfg.log_troubles ? c.log_mode : 0;
     {
       const double log_bytes = ds.log_mode ? 3.0 * (ds.log_mode == 2 ? 2 : 1) * region_bytes(rint, 1, 8) : 0.0;
@@ -458,27 +470,45 @@ int run_stage_t(fvh_handle* h, const StageCall& c, cudaStream_t s) {
                                                                                          sizeof(Tc)) +
                             region_bytes(rint, 1, 1) + log_bytes,
                         s);
-      k_detect<Tc><<<blocks_for(region_points(rint)), 256, 0, s>>>((const Tc*)h->W, rW, (const Tc*)h->Ws,
-                                                                   padded_region(h, 3), rint, ds, h->sc, h->trouble,
-                                                                   h->logs[0], h->logs[1], h->logs[2]);
+      const View<const Tc> vw = make_view((const Tc*)h->W, rW);
+      const View<const Tc> vws = make_view((const Tc*)h->Ws, padded_region(h, 3));
+      const View<uint8_t> vtr = make_view(h->trouble, rint);
+      if (h->ndim == 1)
+        launch_detect<1>(h, vw, vws, bint, ds, vtr, s);
+      else if (h->ndim == 2)
+        launch_detect<2>(h, vw, vws, bint, ds, vtr, s);
+      else
+        launch_detect<3>(h, vw, vws, bint, ds, vtr, s);
     }
     if ((st = set_cuda_error(h, "detect"))) return st;
     if (cfg.convex) {
       if ((st = convex_weights(h, s))) return st;
     }
+    // primitives of the stage input with 2 ghosts, into W (no longer needed)
+    const Region r1 = padded_region(h, 2);
+    {
+      LaunchScope scope(KK_FALLBACK, state_bytes + region_bytes(r1, h->nv, sizeof(Tc)), s);
+      const Box b1 = make_box(r1);
+      k_pointwise_primitives<Tc, NV><<<blocks_for(b1.count), 256, 0, s>>>(c.stage_in, h->grid,
+                                                                          make_view((Tc*)h->W, r1), b1, ph);
+    }
     for (int d = 0; d < 3; ++d) {
       if (!h->active[d]) continue;
       FallbackSpec fb{};
       fb.d = d;
+      fb.nd = h->n[d];
       fb.muscl = h->p[d] > 0 ? 1 : 0;
       fb.limiter = cfg.slope_limiter;
-      fb.rflux = face_region(h, d);
-      fb.rint = rint;
+      const Region rf = face_region(h, d);
       {
         LaunchScope scope(KK_FALLBACK,
-                          region_bytes(rint, 1, 1) + state_bytes + 2 * region_bytes(fb.rflux, h->nv, sizeof(Tc)), s);
-        k_fallback<Tc, NV><<<blocks_for(region_points(fb.rflux)), 256, 0, s>>>(
-            c.stage_in, h->grid, (Tc*)h->F[d], h->trouble, cfg.convex ? h->theta[d] : nullptr, fb, ph);
+                          region_bytes(rint, 1, 1) + region_bytes(r1, h->nv, sizeof(Tc)) +
+                              2 * region_bytes(rf, h->nv, sizeof(Tc)),
+                          s);
+        const Box bf = make_box(rf);
+        k_fallback<Tc, NV><<<blocks_for(bf.count), 256, 0, s>>>(
+            make_view((const Tc*)h->W, r1), make_view((Tc*)h->F[d], rf), bf, make_view((const uint8_t*)h->trouble, rint),
+            cfg.convex ? h->theta[d] : nullptr, fb, ph);
       }
       if ((st = set_cuda_error(h, "fallback"))) return st;
     }
@@ -495,7 +525,8 @@ int run_stage_t(fvh_handle* h, const StageCall& c, cudaStream_t s) {
       default: arrays = 1; break;
     }
     LaunchScope scope(KK_FINAL, flux_bytes + arrays * state_bytes, s);
-    k_final<Tc, NV><<<blocks_for(region_points(rint)), 256, 0, s>>>(rint, fs, ph, c.spec, h->sc);
+    k_final<Tc, NV><<<blocks_for(bint.count), 256, 0, s>>>(bint, make_view((double*)nullptr, rint), fs, ph, c.spec,
+                                                           h->sc);
   }
   return set_cuda_error(h, "final");
 }

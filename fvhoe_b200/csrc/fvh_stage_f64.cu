@@ -32,31 +32,27 @@ __global__ void k_finalize_dt(Scalars* sc, double cfl_h, int use_fixed, double f
   }
 }
 
-__global__ void k_convex_init(const uint8_t* __restrict__ trouble, Region rint, Region rpad, float* __restrict__ th) {
-  const int64_t npts = region_points(rpad);
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < npts;
-       idx += (int64_t)gridDim.x * blockDim.x) {
+__global__ void k_convex_init(View<const uint8_t> trouble, Region rint, Box pad, float* __restrict__ th) {
+  FVH_FOR_POINTS(pad, idx) {
     int i0, i1, i2;
-    region_point(rpad, idx, i0, i1, i2);
+    box_point(pad, idx, i0, i1, i2);
     const bool inside = i0 >= 0 && i0 < rint.n[0] && i1 >= 0 && i1 < rint.n[1] && i2 >= 0 && i2 < rint.n[2];
-    th[idx] = inside ? (float)trouble[region_index(rint, 0, i0, i1, i2)] : 0.0f;
+    th[idx] = inside ? (float)trouble.p[trouble.at(i0, i1, i2)] : 0.0f;
   }
 }
 
 // One statement "theta[target] = max(coef * src[target + shift], theta[target])"
 // of the reference's convex broadcast; src_is_theta turns src into (src > 0).
-__global__ void k_convex_step(const float* __restrict__ src, const float* __restrict__ prev, float* __restrict__ out,
-                              Region rpad, int s0, int s1, int s2, float coef, int src_is_theta) {
-  const int64_t npts = region_points(rpad);
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < npts;
-       idx += (int64_t)gridDim.x * blockDim.x) {
+__global__ void k_convex_step(View<const float> src, const float* __restrict__ prev, float* __restrict__ out, Box pad,
+                              int s0, int s1, int s2, float coef, int src_is_theta) {
+  FVH_FOR_POINTS(pad, idx) {
     int i0, i1, i2;
-    region_point(rpad, idx, i0, i1, i2);
+    box_point(pad, idx, i0, i1, i2);
     const int j0 = i0 + s0, j1 = i1 + s1, j2 = i2 + s2;
     float v = prev[idx];
-    if (j0 >= rpad.lo[0] && j0 < rpad.lo[0] + rpad.n[0] && j1 >= rpad.lo[1] && j1 < rpad.lo[1] + rpad.n[1] &&
-        j2 >= rpad.lo[2] && j2 < rpad.lo[2] + rpad.n[2]) {
-      float x = src[region_index(rpad, 0, j0, j1, j2)];
+    if (j0 >= pad.lo[0] && j0 < pad.lo[0] + pad.n[0] && j1 >= pad.lo[1] && j1 < pad.lo[1] + pad.n[1] &&
+        j2 >= pad.lo[2] && j2 < pad.lo[2] + pad.n[2]) {
+      float x = src.p[src.at(j0, j1, j2)];
       if (src_is_theta) x = x > 0.0f ? 1.0f : 0.0f;
       const float c = coef * x;
       v = c > v ? c : v;
@@ -66,25 +62,23 @@ __global__ void k_convex_step(const float* __restrict__ src, const float* __rest
 }
 
 // Face weight = max(theta of the two cells sharing the face).
-__global__ void k_convex_faces(const float* __restrict__ th, Region rpad, float* __restrict__ theta, Region rflux,
-                               int d) {
-  const int64_t npts = region_points(rflux);
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < npts;
-       idx += (int64_t)gridDim.x * blockDim.x) {
+__global__ void k_convex_faces(View<const float> th, float* __restrict__ theta, Box faces, int d) {
+  const int sd = th.stride(d);
+  FVH_FOR_POINTS(faces, idx) {
     int i0, i1, i2;
-    region_point(rflux, idx, i0, i1, i2);
-    int a0 = i0, a1 = i1, a2 = i2;
-    step_axis(d, -1, a0, a1, a2);
-    const float x = th[region_index(rpad, 0, i0, i1, i2)];
-    const float y = th[region_index(rpad, 0, a0, a1, a2)];
+    box_point(faces, idx, i0, i1, i2);
+    const int o = th.at(i0, i1, i2);
+    const float x = th.p[o];
+    const float y = th.p[o - sd];
     theta[idx] = x > y ? x : y;
   }
 }
 
 int convex_weights(fvh_handle* h, cudaStream_t s) {
-  Region rpad = padded_region(h, 2);
+  const Region rpad = padded_region(h, 2);
   const Region rint = interior_region(h);
-  const unsigned nb = blocks_for(region_points(rpad));
+  const Box pad = make_box(rpad);
+  const unsigned nb = blocks_for(pad.count);
   // conv holds three padded arrays: the trouble flags and two theta buffers
   const int64_t np = region_points(rpad);
   float* t0 = h->conv;
@@ -92,9 +86,9 @@ int convex_weights(fvh_handle* h, cudaStream_t s) {
   float* th_b = h->conv + 2 * np;
   {
     LaunchScope scope(KK_SMALL, 0.0, s);
-    k_convex_init<<<nb, 256, 0, s>>>(h->trouble, rint, rpad, t0);
+    k_convex_init<<<nb, 256, 0, s>>>(make_view((const uint8_t*)h->trouble, rint), rint, pad, t0);
   }
-  cudaMemcpyAsync(th_a, t0, sizeof(float) * region_points(rpad), cudaMemcpyDeviceToDevice, s);
+  cudaMemcpyAsync(th_a, t0, sizeof(float) * np, cudaMemcpyDeviceToDevice, s);
   int ax[3], na = 0;
   for (int a = 0; a < 3; ++a)
     if (h->active[a]) ax[na++] = a;
@@ -121,7 +115,8 @@ int convex_weights(fvh_handle* h, cudaStream_t s) {
     const float* src = list[i].theta_src ? cur : t0;
     {
       LaunchScope scope(KK_SMALL, 0.0, s);
-      k_convex_step<<<nb, 256, 0, s>>>(src, cur, nxt, rpad, sh[0], sh[1], sh[2], list[i].coef, list[i].theta_src);
+      k_convex_step<<<nb, 256, 0, s>>>(make_view(src, rpad), cur, nxt, pad, sh[0], sh[1], sh[2], list[i].coef,
+                                       list[i].theta_src);
     }
     float* tmp = cur;
     cur = nxt;
@@ -129,9 +124,9 @@ int convex_weights(fvh_handle* h, cudaStream_t s) {
   }
   for (int q = 0; q < na; ++q) {
     const int d = ax[q];
-    const Region rf = face_region(h, d);
+    const Box bf = make_box(face_region(h, d));
     LaunchScope scope(KK_SMALL, 0.0, s);
-    k_convex_faces<<<blocks_for(region_points(rf)), 256, 0, s>>>(cur, rpad, h->theta[d], rf, d);
+    k_convex_faces<<<blocks_for(bf.count), 256, 0, s>>>(make_view((const float*)cur, rpad), h->theta[d], bf, d);
   }
   return set_cuda_error(h, "convex weights");
 }
