@@ -83,7 +83,11 @@ class FvhConfig(ctypes.Structure):
         ("precision", ctypes.c_int),
         ("log_troubles", ctypes.c_int),
         ("device", ctypes.c_int),
+        ("kernel_path", ctypes.c_int),
     ]
+
+
+PATH = {"auto": 0, "generic": 1, "fused2d": 2}
 
 
 class FvhStats(ctypes.Structure):

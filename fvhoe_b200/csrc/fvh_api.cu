@@ -181,6 +181,25 @@ int configure(fvh_handle* h, const fvh_config* cfg, std::string& msg) {
     msg = "3D convex broadcast not implemented";
     return FVH_ERR_CONFIG;
   }
+  if (cfg->kernel_path < FVH_PATH_AUTO || cfg->kernel_path > FVH_PATH_FUSED2D) {
+    msg = "unknown kernel path";
+    return FVH_ERR_CONFIG;
+  }
+  if (cfg->kernel_path == FVH_PATH_FUSED2D) {
+    int na = 0, p0 = -1;
+    bool same = true;
+    for (int a = 0; a < 3; ++a) {
+      if (!(cfg->n[a] == 1 && cfg->p[a] == 0)) {
+        ++na;
+        if (p0 < 0) p0 = cfg->p[a];
+        same = same && cfg->p[a] == p0;
+      }
+    }
+    if (na != 2 || cfg->nvars != 5 || (cfg->a_posteriori && cfg->convex) || !same || p0 < 1) {
+      msg = "the fused 2D kernels need two active axes, five variables, equal p in 1..8, no convex weights";
+      return FVH_ERR_CONFIG;
+    }
+  }
   if (cfg->pad_var < -1 || cfg->pad_var > 4) {
     msg = "pad_var must be -1 or a primitive index in [0, 4]";
     return FVH_ERR_CONFIG;

@@ -277,14 +277,19 @@ __global__ void __launch_bounds__(256)
         base += j * state_stride(grid, a);
       }
       const int sa = state_stride(grid, axis);
+      const int ia = axis == 0 ? i[0] : (axis == 1 ? i[1] : i[2]);
+      const int na = axis == 0 ? grid.n[0] : (axis == 1 ? grid.n[1] : grid.n[2]);
+      const int lo_kind = axis == 0 ? grid.bc[0][0] : (axis == 1 ? grid.bc[1][0] : grid.bc[2][0]);
+      const int hi_kind = axis == 0 ? grid.bc[0][1] : (axis == 1 ? grid.bc[1][1] : grid.bc[2][1]);
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         bool fk = false;
-        const int jk = ghost_source(i[axis] + rule.off + k, grid.n[axis], grid.bc[axis][0], grid.bc[axis][1], fk);
+        const int jk = ghost_source(ia + rule.off + k, na, lo_kind, hi_kind, fk);
         const double* q = state + base + jk * sa;
         for (int v = 0; v < nv; ++v) {
           double x = q[v * plane];
-          const bool flip = (v >= 1 && v <= 3) && ((v - 1 == axis) ? fk : fl[v - 1]);
+          const bool flip = (v == 1 && (axis == 0 ? fk : fl[0])) || (v == 2 && (axis == 1 ? fk : fl[1])) ||
+                            (v == 3 && (axis == 2 ? fk : fl[2]));
           if (flip) x = -x;
           acc[v] = acc[v] + rule.w[k] * (Tc)x;
         }
@@ -672,7 +677,7 @@ __global__ void __launch_bounds__(256)
     if (theta_in) {
       theta = (Tc)theta_in[idx];
     } else {
-      const int j = i[d];
+      const int j = d == 0 ? i[0] : (d == 1 ? i[1] : i[2]);
       const int ot = trouble.at(i[0], i[1], i[2]);
       const uint8_t tl = j >= 1 ? trouble.p[ot - st] : 0;
       const uint8_t tr = j < fb.nd ? trouble.p[ot] : 0;

@@ -87,19 +87,25 @@ __device__ __forceinline__ T cfl_speed(const Phys<T>& ph, const T* w, T ndim) {
   return s + ndim * c;
 }
 
+// Component 1 + d of a per-point array, selected without a run-time index so
+// the array stays in registers.
+template <typename T>
+__device__ __forceinline__ T normal_component(const T* w, int d) {
+  return d == 0 ? w[1] : (d == 1 ? w[2] : w[3]);
+}
+
 // Physical Euler flux along axis d (0..2), fvhoe/hydro.py:213-246.
 template <typename T>
 __device__ __forceinline__ void physical_flux(int nv, const T* w, const T* u, int d, bool with_pressure, T* f) {
-  const T v = w[1 + d];
+  const T v = normal_component(w, d);
   f[0] = v * w[0];
-  f[1] = v * u[1];
-  f[2] = v * u[2];
-  f[3] = v * u[3];
-  f[4] = v * u[4];
-  if (with_pressure) {
-    f[1 + d] = f[1 + d] + w[4];
-    f[4] = f[4] + v * w[4];
+#pragma unroll
+  for (int k = 1; k < 4; ++k) {
+    f[k] = v * u[k];
+    if (with_pressure && k - 1 == d) f[k] = f[k] + w[4];
   }
+  f[4] = v * u[4];
+  if (with_pressure) f[4] = f[4] + v * w[4];
   for (int k = 5; k < nv; ++k) f[k] = v * u[k];
 }
 
@@ -118,7 +124,7 @@ __device__ __forceinline__ void riemann_flux(const Phys<T>& ph, int nv, const T*
     T fl[NVA], fr[NVA];
     physical_flux(nv, wl, ul, d, false, fl);
     physical_flux(nv, wr, ur, d, false, fr);
-    const T v = wl[1 + d];
+    const T v = normal_component(wl, d);
     for (int k = 0; k < nv; ++k) out[k] = v > T(0) ? fl[k] : (v < T(0) ? fr[k] : T(0));
     return;
   }
@@ -126,8 +132,8 @@ __device__ __forceinline__ void riemann_flux(const Phys<T>& ph, int nv, const T*
     T fl[NVA], fr[NVA];
     physical_flux(nv, wl, ul, d, true, fl);
     physical_flux(nv, wr, ur, d, true, fr);
-    const T sl = fabs(wl[1 + d]) + sound_speed(ph, wl[0], wl[4]);
-    const T sr = fabs(wr[1 + d]) + sound_speed(ph, wr[0], wr[4]);
+    const T sl = fabs(normal_component(wl, d)) + sound_speed(ph, wl[0], wl[4]);
+    const T sr = fabs(normal_component(wr, d)) + sound_speed(ph, wr[0], wr[4]);
     const T half_smax = T(0.5) * np_maximum(sl, sr);
     for (int k = 0; k < nv; ++k) out[k] = T(0.5) * (fl[k] + fr[k]) - half_smax * (ur[k] - ul[k]);
     return;
@@ -135,7 +141,7 @@ __device__ __forceinline__ void riemann_flux(const Phys<T>& ph, int nv, const T*
   const T cl = sound_speed(ph, wl[0], wl[4]);
   const T cr = sound_speed(ph, wr[0], wr[4]);
   const T cmax = np_maximum(cl, cr);
-  const T vl = wl[1 + d], vr = wr[1 + d];
+  const T vl = normal_component(wl, d), vr = normal_component(wr, d);
   const T rl = wl[0], rr = wr[0];
   const T pl = wl[4], pr = wr[4];
   const T el = ul[4], er = ur[4];
@@ -164,6 +170,7 @@ __device__ __forceinline__ void riemann_flux(const Phys<T>& ph, int nv, const T*
   }
   const T mass = r_g * v_g;
   out[0] = mass;
+#pragma unroll
   for (int t = 0; t < 3; ++t) {
     if (t == d) {
       out[1 + t] = mass * v_g + p_g;

@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <string>
 
+#include "fvh_fused2d.cuh"
 #include "fvh_handle.h"
 #include "fvh_profile.h"
 
@@ -531,8 +532,178 @@ int run_stage_t(fvh_handle* h, const StageCall& c, cudaStream_t s) {
   return set_cuda_error(h, "final");
 }
 
+// ---------------------------------------------------------------------------
+// fused 2D stage (fvh_fused2d.cuh)
+// ---------------------------------------------------------------------------
+// Tile shapes (rows along X x columns along the contiguous Y) per precision.
+template <typename Tc>
+struct FusedTiles;
+template <>
+struct FusedTiles<float> {
+  static constexpr int PX = 16, PY = 32;  // primitives
+  static constexpr int FX = 16, FY = 32;  // fluxes
+  static constexpr int DX = 16, DY = 32;  // detection
+  static constexpr int EX = 16, EY = 32;  // fallback + final
+};
+template <>
+struct FusedTiles<double> {
+  static constexpr int PX = 16, PY = 32;
+  static constexpr int FX = 8, FY = 32;
+  static constexpr int DX = 8, DY = 32;
+  static constexpr int EX = 8, EY = 32;
+};
+
+// Eligible: two active axes, five variables, the same degree 1..8 on both,
+// simple face broadcast.
+inline bool fused2d_eligible(const fvh_handle* h) {
+  if (h->ndim != 2 || h->nv != 5 || h->cfg.convex) return false;
+  int ax[2], na = 0;
+  for (int a = 0; a < 3; ++a)
+    if (h->active[a]) ax[na++] = a;
+  return h->p[ax[0]] == h->p[ax[1]] && h->p[ax[0]] >= 1 && h->p[ax[0]] <= 8;
+}
+
+inline void set_smem(const void* kernel, size_t bytes) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <typename Tc, int P>
+int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
+  using T = FusedTiles<Tc>;
+  constexpr int R = (P + 1) / 2, RC = P / 2;
+  constexpr int KC = 2 * RC + 1, KF = 2 * R + 1;
+  const Phys<Tc> ph = make_phys<Tc>(h);
+  const fvh_config& cfg = h->cfg;
+  const bool apost = cfg.a_posteriori != 0;
+  int ax[2], na = 0;
+  for (int a = 0; a < 3; ++a)
+    if (h->active[a]) ax[na++] = a;
+  f2::Geo g;
+  g.nx = h->n[ax[0]];
+  g.ny = h->n[ax[1]];
+  g.bcx[0] = cfg.bc[ax[0]][0];
+  g.bcx[1] = cfg.bc[ax[0]][1];
+  g.bcy[0] = cfg.bc[ax[1]][0];
+  g.bcy[1] = cfg.bc[ax[1]][1];
+  g.dx = ax[0];
+  g.dy = ax[1];
+  g.gmax = h->gW + 2 * h->r[ax[0]];
+  const Rule<Tc, KC> crule = device_rule<Tc, KC>(centre_rule(P));
+  const Rule<Tc, KC> trule = device_rule<Tc, KC>(transverse_rule(P));
+  const Rule<Tc, KF> lrule = device_rule<Tc, KF>(left_face_rule(P));
+  const Rule<Tc, KF> rrule = device_rule<Tc, KF>(right_face_rule(P));
+  const double cx = h->neg_inv_h[ax[0]], cy = h->neg_inv_h[ax[1]];
+  const double cells = (double)g.nx * g.ny;
+  int st;
+  {
+    LaunchScope scope(KK_SMALL, 0.0, s);
+    k_reset_scalars<<<1, 32, 0, s>>>(h->sc, c.first_stage);
+  }
+  // 1. W with gW ghosts + reductions
+  {
+    using D = f2::PrimsDims<P, T::PX, T::PY>;
+    const size_t smem = (size_t)(D::A + D::B) * sizeof(Tc);
+    auto kern = f2::k2_primitives<Tc, P, T::PX, T::PY, KC, true>;
+    set_smem((const void*)kern, smem);
+    ReduceSpec rs{};
+    rs.cfl = cfg.use_fixed_dt ? 0 : 1;
+    rs.cfl_box = Region{{-h->gw, -h->gw, 0}, {g.nx + 2 * h->gw, g.ny + 2 * h->gw, 1}};
+    rs.extrema = (apost && cfg.nad_global) ? 1 : 0;
+    rs.ext_box = Region{{-3, -3, 0}, {g.nx + 6, g.ny + 6, 1}};
+    rs.ndim = 2.0;
+    const int gw = h->gW;
+    const dim3 grid((g.ny + 2 * gw + T::PY - 1) / T::PY, (g.nx + 2 * gw + T::PX - 1) / T::PX);
+    LaunchScope scope(KK_CENTRE, cells * 5 * (8.0 + sizeof(Tc)), s);
+    kern<<<grid, 256, smem, s>>>(c.stage_in, g, f2::make_v2((Tc*)h->W, g.nx, g.ny, gw), gw, crule, trule, ph, rs,
+                                 h->sc);
+  }
+  if ((st = set_cuda_error(h, "fused primitives"))) return st;
+  {
+    LaunchScope scope(KK_SMALL, 0.0, s);
+    k_finalize_dt<<<1, 1, 0, s>>>(h->sc, h->cfl_h, cfg.use_fixed_dt, cfg.fixed_dt, c.first_stage, c.has_target,
+                                  c.t, c.target);
+  }
+  const f2::V2<Tc> F = f2::make_v2((Tc*)h->F[ax[0]], g.nx + 1, g.ny, 0);
+  const f2::V2<Tc> G = f2::make_v2((Tc*)h->F[ax[1]], g.nx, g.ny + 1, 0);
+  // 2. fluxes (+ candidate)
+  {
+    using D = f2::FluxDims<P, T::FX, T::FY>;
+    const size_t smem = (size_t)(D::SW + D::SA + D::SB + D::SF + D::SG) * sizeof(Tc);
+    auto kern = f2::k2_fluxes<Tc, P, T::FX, T::FY, KC, KF>;
+    set_smem((const void*)kern, smem);
+    const dim3 grid((g.ny + T::FY - 1) / T::FY, (g.nx + T::FX - 1) / T::FX);
+    LaunchScope scope(KK_FACE, cells * 5 * (3.0 * sizeof(Tc) + (apost ? 16.0 : 0.0)), s);
+    f2::V2<const Tc> Wc{(const Tc*)h->W, h->gW, g.ny + 2 * h->gW, (g.nx + 2 * h->gW) * (g.ny + 2 * h->gW)};
+    kern<<<grid, 256, smem, s>>>(Wc, c.stage_in, g, F, G, apost ? h->Us : nullptr, crule, trule, lrule, rrule, ph,
+                                 cx, cy, h->sc);
+  }
+  if ((st = set_cuda_error(h, "fused fluxes"))) return st;
+  // 3. W* + detection
+  if (apost) {
+    DetectSpec ds{};
+    ds.nad_global = cfg.nad_global;
+    ds.nad_relative = cfg.nad_relative;
+    ds.nad_eps = cfg.nad_eps;
+    ds.nad_var_mask = cfg.nad_var_mask;
+    ds.sed = cfg.sed;
+    ds.sed_eps = cfg.sed_eps;
+    ds.pad_var = cfg.pad_var;
+    ds.pad_lo = cfg.pad_lo;
+    ds.pad_hi = cfg.pad_hi;
+    ds.force_trouble = cfg.force_trouble;
+    ds.log_mode = cfg.log_troubles ? c.log_mode : 0;
+    using D = f2::PrimsDims<P, T::DX + 6, T::DY + 6>;
+    const size_t smem = (size_t)(D::A + D::B) * sizeof(Tc);
+    auto kern = f2::k2_detect<Tc, P, T::DX, T::DY, KC>;
+    set_smem((const void*)kern, smem);
+    const dim3 grid((g.ny + T::DY - 1) / T::DY, (g.nx + T::DX - 1) / T::DX);
+    LaunchScope scope(KK_DETECT, cells * (5 * 8.0 + 5 * sizeof(Tc) + 1 + (ds.log_mode ? 48.0 : 0.0)), s);
+    f2::V2<const Tc> Wc{(const Tc*)h->W, h->gW, g.ny + 2 * h->gW, (g.nx + 2 * h->gW) * (g.ny + 2 * h->gW)};
+    kern<<<grid, 256, smem, s>>>(h->Us, g, Wc, crule, trule, ph, ds, h->sc, h->trouble, h->logs[0], h->logs[1],
+                                 h->logs[2]);
+    if ((st = set_cuda_error(h, "fused detect"))) return st;
+  }
+  // 4. fallback + divergence + Runge-Kutta
+  {
+    using D = f2::FinalDims<T::EX, T::EY>;
+    const size_t smem = (size_t)(D::SP + D::SF + D::SG) * sizeof(Tc);
+    auto kern = f2::k2_final<Tc, T::EX, T::EY>;
+    set_smem((const void*)kern, smem);
+    const dim3 grid((g.ny + T::EY - 1) / T::EY, (g.nx + T::EX - 1) / T::EX);
+    int arrays = 1;
+    switch (c.spec.integrator) {
+      case INT_EULER: arrays = 2; break;
+      case INT_SSPRK2: arrays = c.spec.stage == 0 ? 2 : 3; break;
+      case INT_SSPRK3: arrays = c.spec.stage == 1 ? 4 : 3; break;
+      case INT_RK4: arrays = c.spec.stage == 0 ? 3 : (c.spec.stage == 3 ? 3 : 4); break;
+      default: arrays = 1; break;
+    }
+    LaunchScope scope(KK_FINAL, cells * (5 * 2.0 * sizeof(Tc) + arrays * 40.0 + (apost ? 41.0 : 0.0)), s);
+    f2::V2<const Tc> Fc{F.p, 0, F.sx, F.vs};
+    f2::V2<const Tc> Gc{G.p, 0, G.sx, G.vs};
+    kern<<<grid, 256, smem, s>>>(c.stage_in, g, Fc, Gc, h->trouble, apost ? 1 : 0, 1, cfg.slope_limiter, ph, cx, cy,
+                                 c.spec, h->sc);
+  }
+  return set_cuda_error(h, "fused final");
+}
+
 template <typename Tc>
 int run_stage_any(fvh_handle* h, const StageCall& c, cudaStream_t s) {
+  if (h->cfg.kernel_path != FVH_PATH_GENERIC && fused2d_eligible(h)) {
+    int p = 0;
+    for (int a = 0; a < 3; ++a)
+      if (h->active[a]) p = h->p[a];
+    switch (p) {
+      case 1: return run_stage_fused2d<Tc, 1>(h, c, s);
+      case 2: return run_stage_fused2d<Tc, 2>(h, c, s);
+      case 3: return run_stage_fused2d<Tc, 3>(h, c, s);
+      case 4: return run_stage_fused2d<Tc, 4>(h, c, s);
+      case 5: return run_stage_fused2d<Tc, 5>(h, c, s);
+      case 6: return run_stage_fused2d<Tc, 6>(h, c, s);
+      case 7: return run_stage_fused2d<Tc, 7>(h, c, s);
+      case 8: return run_stage_fused2d<Tc, 8>(h, c, s);
+    }
+  }
   if (h->nv == 5) return run_stage_t<Tc, 5>(h, c, s);
   return run_stage_t<Tc, 0>(h, c, s);
 }

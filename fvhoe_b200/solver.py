@@ -1,7 +1,7 @@
 """EulerSolver with the "cuda" array backend.
 
 The constructor takes the arguments of fvhoe/solver.py:42-84 (plus
-`backend`, `precision` and `log_troubles`), builds the mesh and the initial
+`backend`, `precision`, `log_troubles` and `kernel_path`), builds the mesh and the initial
 condition on the host exactly as the reference does (fvhoe/solver.py:220-312),
 moves the state to the GPU once, and from then on every right-hand-side
 evaluation and every time step runs in the CUDA library libfvh.so through its
@@ -77,6 +77,7 @@ class EulerSolver(ODE):
         backend: str = None,
         precision: str = "fp64",
         log_troubles: bool = True,
+        kernel_path: str = "auto",
     ):
         if backend is None:
             backend = os.environ.get("FVHOE_BACKEND", "cuda")
@@ -87,6 +88,9 @@ class EulerSolver(ODE):
         from . import _capi  # raises when libfvh.so is missing
 
         self._capi = _capi
+        if kernel_path not in _capi.PATH:
+            raise ValueError(f"kernel_path must be one of {sorted(_capi.PATH)}")
+        self.kernel_path = kernel_path
         self.backend = backend
         self.precision = precision
         self.csq_floor = csq_floor
@@ -243,6 +247,7 @@ class EulerSolver(ODE):
         cfg.precision = c.PRECISION[self.precision]
         cfg.log_troubles = int(self._log_enabled)
         cfg.device = int(self.am("u").device.index or 0)
+        cfg.kernel_path = c.PATH[self.kernel_path]
         return cfg
 
     def _create_handle(self):

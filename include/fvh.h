@@ -97,7 +97,13 @@ typedef struct fvh_config {
   int precision;     /* FVH_PREC_* */
   int log_troubles;  /* 1: keep the running trouble / NAD / PAD sums used by snapshots */
   int device;        /* CUDA device ordinal the handle's memory and kernels live on */
+  int kernel_path;   /* FVH_PATH_*: which kernel family runs the stage */
 } fvh_config;
+
+/* kernel families (identical results in FP64) */
+#define FVH_PATH_AUTO 0    /* fused 2D tiles when eligible, else the generic passes */
+#define FVH_PATH_GENERIC 1 /* generic N-D passes, any configuration */
+#define FVH_PATH_FUSED2D 2 /* fused 2D tiles; fvh_create refuses ineligible configurations */
 
 typedef struct fvh_handle fvh_handle;
 

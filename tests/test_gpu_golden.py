@@ -25,10 +25,14 @@ def _solver(c, u0, **extra):
     return EulerSolver(**solver_kwargs(c, u0, **extra))
 
 
+KERNEL_PATHS = ["auto", "generic"]
+
+
+@pytest.mark.parametrize("kernel_path", KERNEL_PATHS)
 @pytest.mark.parametrize("path", RHS, ids=[os.path.basename(p) for p in RHS])
-def test_rhs_bit_exact(path):
+def test_rhs_bit_exact(path, kernel_path):
     c, d = load(path)
-    s = _solver(c, d["u0"])
+    s = _solver(c, d["u0"], kernel_path=kernel_path)
     dt, dudt = s.f(0.0, s.am("u"))
     assert dt == float(d["dt"])
     got = dudt.cpu().numpy()
@@ -42,10 +46,11 @@ def test_rhs_bit_exact(path):
         assert np.array_equal(pad[0], d["pad_mag"])
 
 
+@pytest.mark.parametrize("kernel_path", KERNEL_PATHS)
 @pytest.mark.parametrize("path", STEPS, ids=[os.path.basename(p) for p in STEPS])
-def test_steps_bit_exact(path):
+def test_steps_bit_exact(path, kernel_path):
     c, d = load(path)
-    s = _solver(c, d["u0"])
+    s = _solver(c, d["u0"], kernel_path=kernel_path)
     stepper = getattr(s, c["integrator"])
     if "T" in d:
         stepper(float(d["T"]))
@@ -71,3 +76,39 @@ def test_fp32_mode_close_to_fp64():
     r32 = s32.am.get_numpy("u")[0]
     l1 = np.mean(np.abs(r32 - r64))
     assert l1 < 1e-5, l1
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("riemann", ["hllc", "llf"])
+def test_fused2d_equals_generic_fp64(p, riemann):
+    """The fused 2D kernels and the generic passes give identical FP64 steps for every degree."""
+    from fvhoe_b200 import BoundaryCondition, EulerSolver, FourQuadrant2D
+
+    n = (40, 36)
+    kw = dict(w0=FourQuadrant2D(seed=p), nx=n[0], ny=n[1], px=p, py=p, gamma=1.4, riemann_solver=riemann,
+              bc=BoundaryCondition(x="outflow", y=("reflective", "outflow")), a_posteriori_slope_limiting=True,
+              NAD=1e-4, progress_bar=False)
+    fused = EulerSolver(kernel_path="fused2d", **kw)
+    generic = EulerSolver(kernel_path="generic", **kw)
+    fused.ssprk3(n=3)
+    generic.ssprk3(n=3)
+    assert fused.t == generic.t
+    assert np.array_equal(fused.am.get_numpy("u"), generic.am.get_numpy("u"))
+    assert np.array_equal(fused.trouble_flags(), generic.trouble_flags())
+    assert np.array_equal(fused.snapshots[-1]["trouble"], generic.snapshots[-1]["trouble"])
+
+
+@pytest.mark.parametrize("p", [3, 5, 7])
+def test_fused2d_fp32_close_to_generic_fp32(p):
+    from fvhoe_b200 import EulerSolver, KelvinHelmholtzNoise2D
+
+    kw = dict(w0=KelvinHelmholtzNoise2D(n=(64, 64), seed=3), nx=64, ny=64, px=p, py=p, gamma=1.4,
+              a_posteriori_slope_limiting=True, NAD=1e-5, progress_bar=False, precision="fp32")
+    a = EulerSolver(kernel_path="fused2d", **kw)
+    b = EulerSolver(kernel_path="generic", **kw)
+    dta, ka = a.f(0.0, a.am("u"))
+    dtb, kb = b.f(0.0, b.am("u"))
+    assert abs(dta - dtb) <= 1e-6 * dtb
+    diff = (ka - kb).abs().max().item()
+    scale = kb.abs().max().item()
+    assert diff <= 1e-4 * scale, (diff, scale)
