@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-sample", type=int, default=512, help="side of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain fp64 comparison (profiling runs)")
     return ap.parse_args()
 
 
@@ -293,7 +294,7 @@ def run_ours(args):
     # the L1 density error of the chosen form against FP64
     chosen = EulerSolver(precision=args.precision, **solver_kwargs(args.n, args.p, seed=rank))
     plain = EulerSolver(precision="fp64", **solver_kwargs(args.n, args.p, seed=rank)) \
-        if args.precision != "fp64" else None
+        if args.precision != "fp64" and not args.no_plain else None
     t_acc = args.accuracy_time
     chosen.ssprk3(t_acc)
     l1 = {"value": 0.0, "t": t_acc, "steps_chosen": chosen.step_count}
