@@ -48,6 +48,14 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=512, help="side of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain fp64 comparison (profiling runs)")
+    ap.add_argument("--no-predictor", action="store_true", help="skip the learned-predictor leg")
+    ap.add_argument("--pred-n", type=int, default=4096, help="cells per side of the learned-predictor leg")
+    ap.add_argument("--pred-p", type=int, default=7)
+    ap.add_argument("--pred-steps", type=int, default=10, help="timed steps of each form in the predictor leg")
+    ap.add_argument("--pred-train-n", type=int, default=1024, help="side of the training runs")
+    ap.add_argument("--pred-snapshots", type=int, default=16, help="stages sampled per training run")
+    ap.add_argument("--pred-epochs", type=int, default=2)
+    ap.add_argument("--pred-accuracy-time", type=float, default=0.002)
     return ap.parse_args()
 
 
@@ -274,6 +282,114 @@ def _time_steps(lib, _capi, h, uptr, sp, stream, steps):
     return ev0.elapsed_time(ev1), step
 
 
+def predictor_leg(args, stream, sp):
+    """The learned troubled-cell predictor on KH at pred_n^2, p = pred_p, FP32 fused.
+
+    1. Training rows from the plain FP64 solver: KH runs of two seeds and a
+       four-quadrant Riemann run at pred_train_n^2, one right-hand-side
+       evaluation every other step (features of every cell + its a-posteriori flag).
+    2. Training on the GPU by the library's tensor-core kernels (Adam, BCE with
+       positives weighted by the class ratio), held-out rates on a KH run of
+       another seed.
+    3. The same initial state advanced to a common time by the plain FP64 path,
+       the FP32 fused path and the FP32 fused path with the predictor: L1 density
+       errors against FP64, miss and false-alarm rates over those steps.
+    4. Timed steps of each form (CUDA events, device-resident state)."""
+    import ctypes
+
+    import torch
+
+    from fvhoe_b200 import (BoundaryCondition, EulerSolver, FourQuadrant2D, TroubledCellPredictor, _capi,
+                            collect_training_data)
+
+    lib = _capi.lib
+    nt = args.pred_train_n
+    every = 2
+    steps = args.pred_snapshots * every
+    t0 = time.perf_counter()
+    runs = [EulerSolver(**solver_kwargs(nt, args.pred_p, seed=101)),
+            EulerSolver(**solver_kwargs(nt, args.pred_p, seed=102)),
+            EulerSolver(w0=FourQuadrant2D(seed=103), nx=nt, ny=nt, px=args.pred_p, py=args.pred_p, gamma=1.4,
+                        riemann_solver="hllc", CFL=0.8, bc=BoundaryCondition(x="outflow", y="outflow"),
+                        a_posteriori_slope_limiting=True, NAD=1e-5, progress_bar=False)]
+    X, y = collect_training_data(runs, steps=steps, every=every)
+    del runs
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    net = TroubledCellPredictor(device=torch.cuda.current_device(), seed=7)
+    t0 = time.perf_counter()
+    hist = net.fit(X, y, epochs=args.pred_epochs, batch=65536, lr=2e-3)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    rows = int(X.shape[0])
+    positives = float(y.float().mean().item())
+    del X, y
+    held = EulerSolver(**solver_kwargs(nt, args.pred_p, seed=104))
+    Xh, yh = collect_training_data([held], steps=8, every=4)
+    held_rates = net.evaluate(Xh, yh, threshold=0.5)
+    del Xh, yh, held
+
+    n, p = args.pred_n, args.pred_p
+    cells = n * n
+
+    def make(precision, with_pred):
+        s = EulerSolver(precision=precision, **solver_kwargs(n, p, seed=0))
+        if with_pred:
+            s.set_predictor(net, threshold=0.5)
+        return s
+
+    plain = make("fp64", False)
+    fused = make("fp32", False)
+    learned = make("fp32", True)
+    t_acc = args.pred_accuracy_time
+    for s in (plain, fused, learned):
+        s.ssprk3(t_acc)
+    rho = plain.am("u")[0]
+    l1_fused = float(torch.mean(torch.abs(fused.am("u")[0] - rho)).item())
+    l1_learned = float(torch.mean(torch.abs(learned.am("u")[0] - rho)).item())
+    rates = learned.predictor_rates()
+
+    def timed(s):
+        h = s._handle
+        up = ctypes.c_void_p(s.am("u").data_ptr())
+        _time_steps(lib, _capi, h, up, sp, stream, args.warmup)
+        ms, _ = _time_steps(lib, _capi, h, up, sp, stream, args.pred_steps)
+        return 3 * cells * args.pred_steps / (ms / 1e3) / 1e6, ms / args.pred_steps
+
+    v_plain, ms_plain = timed(plain)
+    v_fused, ms_fused = timed(fused)
+    v_learned, ms_learned = timed(learned)
+    # kernel shares of the predictor form
+    h = learned._handle
+    _capi.check(lib.fvh_profile_enable(h, 1), h)
+    up = ctypes.c_void_p(learned.am("u").data_ptr())
+    _, step = _time_steps(lib, _capi, h, up, sp, stream, 2)
+    K = len(_capi.KERNEL_KINDS)
+    pms = (ctypes.c_double * K)()
+    plaunch = (ctypes.c_uint64 * K)()
+    _capi.check(lib.fvh_profile_read(h, pms, None, plaunch, sp), h)
+    _capi.check(lib.fvh_profile_enable(h, 0), h)
+    shares = {nm: pms[i] / sum(pms) for i, nm in enumerate(_capi.KERNEL_KINDS) if plaunch[i]}
+    errors = net.errors()
+    return {
+        "config": f"2D Kelvin-Helmholtz {n}x{n}, p={p}, HLLC, SSP-RK3, CFL 0.8, NAD 1e-5 + PAD + SED, periodic",
+        "network": "100 -> 64 -> 64 -> 1 GELU, BF16 tensor-core operands (tcgen05), FP32 accumulation",
+        "training": {"rows": rows, "positive_fraction": positives, "epochs": args.pred_epochs,
+                     "loss_per_epoch": hist, "data_seconds": t_data, "train_seconds": t_train,
+                     "source": f"plain FP64 solver, KH seeds 101/102 and a four-quadrant run at {nt}^2, "
+                               f"p={args.pred_p}, one stage every {every} steps over {steps} steps",
+                     "held_out": held_rates},
+        "mcell_updates_per_s": {"plain_fp64": v_plain, "fp32_fused": v_fused, "fp32_fused_learned": v_learned},
+        "ms_per_step": {"plain_fp64": ms_plain, "fp32_fused": ms_fused, "fp32_fused_learned": ms_learned},
+        "speedup_vs_plain_fp64": {"fp32_fused": v_fused / v_plain, "fp32_fused_learned": v_learned / v_plain},
+        "l1_density_error_vs_fp64": {"t": t_acc, "steps": plain.step_count, "fp32_fused": l1_fused,
+                                     "fp32_fused_learned": l1_learned},
+        "rates_over_l1_run": rates,
+        "kernel_shares_learned": shares,
+        "tensor_core_wait_errors": errors,
+    }
+
+
 def run_ours(args):
     import ctypes
 
@@ -408,6 +524,10 @@ def run_ours(args):
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_port(args)
+        if world == 1 and not args.no_predictor:
+            del chosen
+            torch.cuda.empty_cache()
+            line["learned_predictor"] = predictor_leg(args, stream, sp)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -45,5 +45,16 @@ __all__ = [
     "Sinus",
     "Square",
     "Timer",
+    "TroubledCellPredictor",
     "advection_dt",
+    "collect_training_data",
 ]
+
+
+def __getattr__(name):
+    # the predictor module binds libfvh.so at import; load it on first use
+    if name in ("TroubledCellPredictor", "collect_training_data"):
+        from . import predictor
+
+        return getattr(predictor, name)
+    raise AttributeError(f"module {__name__!r} has no attribute {name!r}")

@@ -46,9 +46,26 @@ EXPORTS = (
     "fvh_primitives_noalloc",
     "fvh_primitives_noalloc_max_doubles",
     "fvh_primitives_noalloc_error",
+    "fvh_mlp_param_count",
+    "fvh_mlp_create",
+    "fvh_mlp_destroy",
+    "fvh_mlp_last_error",
+    "fvh_mlp_get_params",
+    "fvh_mlp_set_params",
+    "fvh_mlp_features",
+    "fvh_mlp_train_step",
+    "fvh_mlp_gradients",
+    "fvh_mlp_logits",
+    "fvh_mlp_errors",
+    "fvh_set_predictor",
+    "fvh_get_pred_stats",
+    "fvh_pred_flags",
 )
 
-KERNEL_KINDS = ("centre", "transverse", "face", "candidate", "detect", "fallback", "final", "small")
+KERNEL_KINDS = ("centre", "transverse", "face", "candidate", "detect", "fallback", "final", "small", "predict")
+
+MLP_FEATURES = 100
+MLP_ROW = 112
 
 
 class FvhConfig(ctypes.Structure):
@@ -101,6 +118,17 @@ class FvhStats(ctypes.Structure):
     ]
 
 
+class FvhPredStats(ctypes.Structure):
+    """Mirror of struct fvh_pred_stats (include/fvh.h)."""
+
+    _fields_ = [
+        ("predicted", ctypes.c_uint),
+        ("troubled", ctypes.c_uint),
+        ("missed", ctypes.c_uint),
+        ("false_alarm", ctypes.c_uint),
+    ]
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
@@ -135,8 +163,29 @@ def _load():
     lib.fvh_primitives_noalloc_max_doubles.restype = ctypes.c_size_t
     lib.fvh_primitives_noalloc_error.argtypes = []
     lib.fvh_primitives_noalloc_error.restype = ctypes.c_char_p
+    fp = ctypes.POINTER(ctypes.c_float)
+    lib.fvh_mlp_param_count.argtypes = []
+    lib.fvh_mlp_param_count.restype = ctypes.c_size_t
+    lib.fvh_mlp_create.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(vp)]
+    lib.fvh_mlp_destroy.argtypes = [vp]
+    lib.fvh_mlp_last_error.argtypes = [vp]
+    lib.fvh_mlp_last_error.restype = ctypes.c_char_p
+    lib.fvh_mlp_get_params.argtypes = [vp, fp, ctypes.c_size_t]
+    lib.fvh_mlp_set_params.argtypes = [vp, fp, ctypes.c_size_t]
+    lib.fvh_mlp_features.argtypes = [vp, vp, vp, vp]
+    lib.fvh_mlp_train_step.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_float, ctypes.c_float, fp, vp]
+    lib.fvh_mlp_gradients.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_float, vp, fp, vp]
+    lib.fvh_mlp_logits.argtypes = [vp, vp, ctypes.c_int, vp, vp]
+    lib.fvh_mlp_errors.argtypes = [vp]
+    lib.fvh_mlp_errors.restype = ctypes.c_uint
+    lib.fvh_set_predictor.argtypes = [vp, vp, ctypes.c_float]
+    lib.fvh_get_pred_stats.argtypes = [vp, ctypes.POINTER(FvhPredStats), vp]
+    lib.fvh_pred_flags.argtypes = [vp, vp, vp]
     for name in ("fvh_create", "fvh_destroy", "fvh_rhs", "fvh_step", "fvh_primitives", "fvh_trouble_flags",
-                 "fvh_trouble_log", "fvh_set_log_mode", "fvh_get_stats", "fvh_profile_enable", "fvh_profile_read"):
+                 "fvh_trouble_log", "fvh_set_log_mode", "fvh_get_stats", "fvh_profile_enable", "fvh_profile_read",
+                 "fvh_mlp_create", "fvh_mlp_destroy", "fvh_mlp_get_params", "fvh_mlp_set_params", "fvh_mlp_features",
+                 "fvh_mlp_train_step", "fvh_mlp_gradients", "fvh_mlp_logits", "fvh_set_predictor",
+                 "fvh_get_pred_stats", "fvh_pred_flags"):
         getattr(lib, name).restype = ctypes.c_int
     return lib
 

@@ -33,6 +33,8 @@ UNITS = {
     # the FP32 path is never compared bit for bit: fast division, square root and FTZ
     "fvh_stage_f32.cu": ["-fmad=true", "--use_fast_math"],
     "fvh_noalloc.cu": ["-fmad=false"],
+    # learned troubled-cell predictor (tensor cores, FP32 epilogues)
+    "fvh_mlp.cu": [],
 }
 
 

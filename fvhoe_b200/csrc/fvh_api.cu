@@ -270,7 +270,7 @@ void release(fvh_handle* h) {
   h->prof = nullptr;
   void* ptrs[] = {h->bufA, h->bufB, h->W,        h->Ws,       h->Us,       h->F[0],     h->F[1],
                   h->F[2], h->trouble, h->logs[0], h->logs[1], h->logs[2], h->acc,      h->S[0],
-                  h->S[1], h->theta[0], h->theta[1], h->theta[2], h->conv, h->sc};
+                  h->S[1], h->theta[0], h->theta[1], h->theta[2], h->conv, h->sc, h->pred};
   for (void* p : ptrs)
     if (p) cudaFree(p);
 }
@@ -561,6 +561,32 @@ int fvh_get_stats(fvh_handle* h, fvh_stats* out, void* stream) {
   out->dt_step = host.dt_step;
   out->troubled = host.troubled;
   out->nonfinite = host.nonfinite;
+  return FVH_OK;
+}
+
+int fvh_get_pred_stats(fvh_handle* h, fvh_pred_stats* out, void* stream) {
+  if (!h || !out) return FVH_ERR_ARG;
+  if (int st0 = use_device(h)) return st0;
+  fvh::Scalars host{};
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(&host, h->sc, sizeof(host), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail(h, FVH_ERR_CUDA, cudaGetErrorString(e));
+  out->predicted = host.predicted;
+  out->troubled = host.judged;
+  out->missed = host.missed;
+  out->false_alarm = host.false_alarm;
+  return FVH_OK;
+}
+
+int fvh_pred_flags(fvh_handle* h, uint8_t* flags, void* stream) {
+  if (!h) return FVH_ERR_ARG;
+  if (!flags) return fail(h, FVH_ERR_ARG, "null array");
+  if (!h->pred) return fail(h, FVH_ERR_CONFIG, "no predictor was attached");
+  if (int st0 = use_device(h)) return st0;
+  const size_t n = (size_t)h->n[0] * h->n[1] * h->n[2];
+  const cudaError_t e = cudaMemcpyAsync(flags, h->pred, n, cudaMemcpyDeviceToDevice, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(h, FVH_ERR_CUDA, cudaGetErrorString(e));
   return FVH_OK;
 }
 

@@ -72,6 +72,68 @@ __device__ __forceinline__ void load_state2(const double* __restrict__ u, const 
   }
 }
 
+// Fallback flux at a face from the pointwise primitives of the four cells
+// around it: element e of variable v at base[v * vstride + e * estride], cells
+// i-2, i-1 | i, i+1. MUSCL with the limiter (fvhoe/slope_limiting.py:24-53),
+// the unlimited p=1 faces, or first order (muscl = 0).
+template <typename Tc>
+__device__ __forceinline__ void fallback_face_flux(const Tc* base, int vstride, int estride, int muscl, int limiter,
+                                                   const Phys<Tc>& ph, int dir, Tc* flo) {
+  Tc wl[5], wr[5];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) {
+    const Tc* pv = base + v * vstride;
+    const Tc a0 = pv[0], a1 = pv[estride], a2 = pv[2 * estride], a3 = pv[3 * estride];
+    if (muscl && limiter == LIMITER_NONE) {
+      wl[v] = ((Tc(0) + Tc(-0.25) * a0) + Tc(1) * a1) + Tc(0.25) * a2;
+      wr[v] = ((Tc(0) + Tc(0.25) * a1) + Tc(1) * a2) + Tc(-0.25) * a3;
+    } else if (muscl) {
+      const Tc sl = limited_slope(a1 - a0, a2 - a1, limiter);
+      const Tc sr = limited_slope(a2 - a1, a3 - a2, limiter);
+      wl[v] = a1 + Tc(0.5) * sl;
+      wr[v] = a2 - Tc(0.5) * sr;
+    } else {
+      wl[v] = a1;
+      wr[v] = a2;
+    }
+  }
+  riemann_flux<5>(ph, 5, wl, wr, dir, flo);
+}
+
+// Pointwise primitives of the stage input on [x0-2, x0+TX+2) x [y0-2, y0+TY+2)
+// into Pw ((TX+4) x (TY+4) per variable), the inputs of the fallback fluxes
+// (p = 1 reconstruction is the identity, fvhoe/solver.py:710-732).
+template <typename Tc, int TX, int TY>
+__device__ __forceinline__ void pointwise_tile(const double* __restrict__ u, const Geo& g, int x0, int y0, Tc* Pw,
+                                               const Phys<Tc>& ph) {
+  constexpr int PX = TX + 4, PY = TY + 4;
+  for (int i = threadIdx.x; i < PX * PY; i += blockDim.x) {
+    const int r = i / PY, q = i - r * PY;
+    Tc uc[5], w[5];
+    load_state2<Tc>(u, g, x0 - 2 + r, y0 - 2 + q, uc);
+    to_primitives(ph, 5, uc, w);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) Pw[(v * PX + r) * PY + q] = w[v];
+  }
+}
+
+// 1 in every thread of the block when a[c] && !b[c] (b nullable) holds for a
+// grid cell c of [x0-1, x0+TX] x [y0-1, y0+TY].
+template <int TX, int TY>
+__device__ __forceinline__ int tile_any(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b, const Geo& g,
+                                        int x0, int y0) {
+  int local = 0;
+  for (int i = threadIdx.x; i < (TX + 2) * (TY + 2); i += blockDim.x) {
+    const int r = i / (TY + 2), q = i - r * (TY + 2);
+    const int x = x0 - 1 + r, y = y0 - 1 + q;
+    if (x >= 0 && x < g.nx && y >= 0 && y < g.ny) {
+      const int o = x * g.ny + y;
+      local |= (a[o] && !(b && b[o])) ? 1 : 0;
+    }
+  }
+  return __syncthreads_or(local);
+}
+
 template <int a, int b>
 struct Max {
   static constexpr int value = a > b ? a : b;
@@ -274,7 +336,7 @@ template <typename Tc, int P, int TX, int TY, int KC, int KF>
 __global__ void __launch_bounds__(256)
     k2_fluxes(V2<const Tc> W, const double* __restrict__ u, Geo g, V2<Tc> F, V2<Tc> G, double* __restrict__ ustar,
               Rule<Tc, KC> c, Rule<Tc, KC> t, Rule<Tc, KF> lrule, Rule<Tc, KF> rrule, Phys<Tc> ph, double cx,
-              double cy, const Scalars* __restrict__ sc) {
+              double cy, const Scalars* __restrict__ sc, const uint8_t* __restrict__ pred, int muscl, int limiter) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   using D = FluxDims<P, TX, TY>;
   constexpr int R = D::R, RC = D::RC, H = D::H;
@@ -429,6 +491,38 @@ __global__ void __launch_bounds__(256)
       ustar[v * plane + o] = u[v * plane + o] + dt * (double)d;
     }
   }
+  // predicted cells: their faces take the fallback flux now, blended as the
+  // final pass would (the candidate above keeps the high-order fluxes)
+  if (!pred || !tile_any<TX, TY>(pred, nullptr, g, x0, y0)) return;
+  constexpr int PWX = TX + 4, PWY = TY + 4;
+  static_assert(PWX * PWY * 5 <= D::SW, "pointwise tile must fit in the W tile");
+  Tc* Pw = Ws;
+  pointwise_tile<Tc, TX, TY>(u, g, x0, y0, Pw, ph);
+  __syncthreads();
+  for (int i = threadIdx.x; i < (TX + 1) * TY; i += nt) {
+    const int f = i / TY, q = i - f * TY;
+    const int x = x0 + f, y = y0 + q;
+    const bool owned = (f < TX || x == g.nx) && x <= g.nx && y < g.ny;
+    if (!owned) continue;
+    if (!((x >= 1 && pred[(x - 1) * g.ny + y]) || (x < g.nx && pred[x * g.ny + y]))) continue;
+    Tc flo[5];
+    fallback_face_flux<Tc>(Pw + f * PWY + q + 2, PWX * PWY, PWY, muscl, limiter, ph, g.dx, flo);
+    Tc* o = F.p + F.at(x, y);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) o[v * F.vs] = (Tc(1) - Tc(1)) * FX[(v * (TX + 1) + f) * TY + q] + Tc(1) * flo[v];
+  }
+  for (int i = threadIdx.x; i < TX * (TY + 1); i += nt) {
+    const int r = i / (TY + 1), f = i - r * (TY + 1);
+    const int x = x0 + r, y = y0 + f;
+    const bool owned = (f < TY || y == g.ny) && y <= g.ny && x < g.nx;
+    if (!owned) continue;
+    if (!((y >= 1 && pred[x * g.ny + y - 1]) || (y < g.ny && pred[x * g.ny + y]))) continue;
+    Tc flo[5];
+    fallback_face_flux<Tc>(Pw + (r + 2) * PWY + f, PWX * PWY, 1, muscl, limiter, ph, g.dy, flo);
+    Tc* o = G.p + G.at(x, y);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) o[v * G.vs] = (Tc(1) - Tc(1)) * GY[(v * TX + r) * (TY + 1) + f] + Tc(1) * flo[v];
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -555,14 +649,13 @@ struct FinalDims {
 template <typename Tc, int TX, int TY>
 __global__ void __launch_bounds__(256)
     k2_final(const double* __restrict__ stage_in, Geo g, V2<const Tc> F, V2<const Tc> G,
-             const uint8_t* __restrict__ trouble, int apost, int muscl, int limiter, Phys<Tc> ph, double cx, double cy,
-             StageSpec st, Scalars* __restrict__ sc) {
+             const uint8_t* __restrict__ trouble, const uint8_t* __restrict__ pred, int apost, int muscl, int limiter,
+             Phys<Tc> ph, double cx, double cy, StageSpec st, Scalars* __restrict__ sc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   using D = FinalDims<TX, TY>;
   Tc* Pw = reinterpret_cast<Tc*>(smem_raw);
   Tc* FX = Pw + D::SP;
   Tc* GY = FX + D::SF;
-  __shared__ int any_trouble;
   const int nt = blockDim.x;
   const int x0 = blockIdx.y * TX, y0 = blockIdx.x * TY;
   // high-order fluxes of the tile's faces
@@ -580,93 +673,44 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int v = 0; v < 5; ++v) GY[(v * TX + r) * (TY + 1) + f] = p[v * G.vs];
   }
-  if (apost) {
-    if (threadIdx.x == 0) any_trouble = 0;
+  // fallback at the faces of troubled cells; with predicted flags, faces next
+  // to a predicted cell already hold their fallback flux (k2_fluxes) and only
+  // the faces of missed cells are revised here
+  if (apost && tile_any<TX, TY>(trouble, pred, g, x0, y0)) {
+    pointwise_tile<Tc, TX, TY>(stage_in, g, x0, y0, Pw, ph);
     __syncthreads();
-    // pointwise primitives with 2 ghosts, and whether the tile touches any troubled cell
-    int local_any = 0;
-    for (int i = threadIdx.x; i < D::PX * D::PY; i += nt) {
-      const int r = i / D::PY, q = i - r * D::PY;
-      const int x = x0 - 2 + r, y = y0 - 2 + q;
-      Tc uc[5], w[5];
-      load_state2<Tc>(stage_in, g, x, y, uc);
-      to_primitives(ph, 5, uc, w);
+    // X faces
+    for (int i = threadIdx.x; i < (TX + 1) * TY; i += nt) {
+      const int f = i / TY, q = i - f * TY;
+      const int x = x0 + f, y = y0 + q;
+      if (x > g.nx || y >= g.ny) continue;
+      const int ol = (x - 1) * g.ny + y, orr = x * g.ny + y;
+      const bool tl = x >= 1 && trouble[ol], trr = x < g.nx && trouble[orr];
+      if (!(tl || trr)) continue;
+      if (pred && ((x >= 1 && pred[ol]) || (x < g.nx && pred[orr]))) continue;
+      Tc flo[5];
+      fallback_face_flux<Tc>(Pw + f * D::PY + q + 2, D::PX * D::PY, D::PY, muscl, limiter, ph, g.dx, flo);
 #pragma unroll
-      for (int v = 0; v < 5; ++v) Pw[(v * D::PX + r) * D::PY + q] = w[v];
-      if (x >= x0 - 1 && x <= x0 + TX && y >= y0 - 1 && y <= y0 + TY && x >= 0 && x < g.nx && y >= 0 &&
-          y < g.ny)
-        local_any |= trouble[x * g.ny + y];
-    }
-    if (local_any) any_trouble = 1;
-    __syncthreads();
-    if (any_trouble) {
-      // X faces
-      for (int i = threadIdx.x; i < (TX + 1) * TY; i += nt) {
-        const int f = i / TY, q = i - f * TY;
-        const int x = x0 + f, y = y0 + q;
-        if (x > g.nx || y >= g.ny) continue;
-        const uint8_t tl = x >= 1 ? trouble[(x - 1) * g.ny + y] : 0;
-        const uint8_t trr = x < g.nx ? trouble[x * g.ny + y] : 0;
-        if (!(tl || trr)) continue;
-        Tc wl[5], wr[5];
-#pragma unroll
-        for (int v = 0; v < 5; ++v) {
-          const Tc* pv = Pw + (v * D::PX + f) * D::PY + q + 2;  // row f = cell x-2
-          const Tc a0 = pv[0], a1 = pv[D::PY], a2 = pv[2 * D::PY], a3 = pv[3 * D::PY];
-          if (muscl && limiter == LIMITER_NONE) {
-            wl[v] = ((Tc(0) + Tc(-0.25) * a0) + Tc(1) * a1) + Tc(0.25) * a2;
-            wr[v] = ((Tc(0) + Tc(0.25) * a1) + Tc(1) * a2) + Tc(-0.25) * a3;
-          } else if (muscl) {
-            const Tc sl = limited_slope(a1 - a0, a2 - a1, limiter);
-            const Tc sr = limited_slope(a2 - a1, a3 - a2, limiter);
-            wl[v] = a1 + Tc(0.5) * sl;
-            wr[v] = a2 - Tc(0.5) * sr;
-          } else {
-            wl[v] = a1;
-            wr[v] = a2;
-          }
-        }
-        Tc flo[5];
-        riemann_flux<5>(ph, 5, wl, wr, g.dx, flo);
-#pragma unroll
-        for (int v = 0; v < 5; ++v) {
-          Tc& fh = FX[(v * (TX + 1) + f) * TY + q];
-          fh = (Tc(1) - Tc(1)) * fh + Tc(1) * flo[v];
-        }
+      for (int v = 0; v < 5; ++v) {
+        Tc& fh = FX[(v * (TX + 1) + f) * TY + q];
+        fh = (Tc(1) - Tc(1)) * fh + Tc(1) * flo[v];
       }
-      // Y faces
-      for (int i = threadIdx.x; i < TX * (TY + 1); i += nt) {
-        const int r = i / (TY + 1), f = i - r * (TY + 1);
-        const int x = x0 + r, y = y0 + f;
-        if (x >= g.nx || y > g.ny) continue;
-        const uint8_t tl = y >= 1 ? trouble[x * g.ny + y - 1] : 0;
-        const uint8_t trr = y < g.ny ? trouble[x * g.ny + y] : 0;
-        if (!(tl || trr)) continue;
-        Tc wl[5], wr[5];
+    }
+    // Y faces
+    for (int i = threadIdx.x; i < TX * (TY + 1); i += nt) {
+      const int r = i / (TY + 1), f = i - r * (TY + 1);
+      const int x = x0 + r, y = y0 + f;
+      if (x >= g.nx || y > g.ny) continue;
+      const int ol = x * g.ny + y - 1, orr = x * g.ny + y;
+      const bool tl = y >= 1 && trouble[ol], trr = y < g.ny && trouble[orr];
+      if (!(tl || trr)) continue;
+      if (pred && ((y >= 1 && pred[ol]) || (y < g.ny && pred[orr]))) continue;
+      Tc flo[5];
+      fallback_face_flux<Tc>(Pw + (r + 2) * D::PY + f, D::PX * D::PY, 1, muscl, limiter, ph, g.dy, flo);
 #pragma unroll
-        for (int v = 0; v < 5; ++v) {
-          const Tc* pv = Pw + (v * D::PX + r + 2) * D::PY + f;  // col f = cell y-2
-          const Tc a0 = pv[0], a1 = pv[1], a2 = pv[2], a3 = pv[3];
-          if (muscl && limiter == LIMITER_NONE) {
-            wl[v] = ((Tc(0) + Tc(-0.25) * a0) + Tc(1) * a1) + Tc(0.25) * a2;
-            wr[v] = ((Tc(0) + Tc(0.25) * a1) + Tc(1) * a2) + Tc(-0.25) * a3;
-          } else if (muscl) {
-            const Tc sl = limited_slope(a1 - a0, a2 - a1, limiter);
-            const Tc sr = limited_slope(a2 - a1, a3 - a2, limiter);
-            wl[v] = a1 + Tc(0.5) * sl;
-            wr[v] = a2 - Tc(0.5) * sr;
-          } else {
-            wl[v] = a1;
-            wr[v] = a2;
-          }
-        }
-        Tc flo[5];
-        riemann_flux<5>(ph, 5, wl, wr, g.dy, flo);
-#pragma unroll
-        for (int v = 0; v < 5; ++v) {
-          Tc& fh = GY[(v * TX + r) * (TY + 1) + f];
-          fh = (Tc(1) - Tc(1)) * fh + Tc(1) * flo[v];
-        }
+      for (int v = 0; v < 5; ++v) {
+        Tc& fh = GY[(v * TX + r) * (TY + 1) + f];
+        fh = (Tc(1) - Tc(1)) * fh + Tc(1) * flo[v];
       }
     }
   }

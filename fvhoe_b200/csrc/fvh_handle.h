@@ -42,6 +42,12 @@ struct fvh_handle {
   fvh::Scalars* sc = nullptr;
   size_t scratch_bytes = 0;
 
+  // learned troubled-cell predictor (optional)
+  fvh_mlp* mlp = nullptr;         // attached network (not owned)
+  uint8_t* pred = nullptr;        // predicted flags of the last stage
+  float pred_thr_logit = 0.0f;    // logit threshold
+  bool last_stage_fused = false;  // the last stage ran the fused 2D kernels
+
   int log_mode_next = 1;          // log mode of the next stage
   fvh::Profiler* prof = nullptr;  // per-launch timing, when enabled
   fvh::KernelTotals prof_totals{};
@@ -66,5 +72,13 @@ int run_stage_f32(fvh_handle* h, const StageCall& c, cudaStream_t s);
 
 // FV primitives of u over the interior (snapshot conversion).
 int primitives_f64(fvh_handle* h, const double* u, double* w, int fv_average, cudaStream_t s);
+
+// Predicted flags h->pred of the stage from h->W (fused 2D layout, after the
+// primitive pass and its extrema reduction).
+int mlp_predict_stage(fvh_handle* h, cudaStream_t s);
+
+// Adds the stage's predicted / troubled / missed / false-alarm counts to the
+// step's predictor statistics (after the detection).
+int mlp_count_stage(fvh_handle* h, cudaStream_t s);
 
 }  // namespace fvh

@@ -203,7 +203,11 @@ struct Scalars {
   double dt_step;                         // the step's dt after the target clamp
   unsigned int troubled;                  // troubled cells found this stage
   unsigned int nonfinite;                 // cells whose update is not finite
-  unsigned int pad_[2];
+  // learned-predictor counts, summed over the stages of a step
+  unsigned int predicted;                 // cells the network flagged
+  unsigned int judged;                    // cells the a-posteriori check flagged
+  unsigned int missed;                    // judged, not predicted
+  unsigned int false_alarm;               // predicted, not judged
 };
 
 // Reduction request for the last transverse sweep of the primitive pass.
@@ -240,6 +244,7 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long x)
 __device__ __forceinline__ void block_count_add(unsigned int count, unsigned int* dst) {
   __shared__ unsigned int s_count[8];
   for (int o = 16; o > 0; o >>= 1) count += __shfl_xor_sync(0xffffffffu, count, o);
+  __syncthreads();  // a previous call's reads of s_count are done
   if ((threadIdx.x & 31) == 0) s_count[threadIdx.x >> 5] = count;
   __syncthreads();
   if (threadIdx.x == 0) {

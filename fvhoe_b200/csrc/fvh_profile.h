@@ -24,6 +24,7 @@ enum KernelKind : int {
   KK_FALLBACK,       // MUSCL fallback + blend
   KK_FINAL,          // divergence + Runge-Kutta combination
   KK_SMALL,          // scalars, convex weights, log arithmetic
+  KK_PREDICT,        // learned troubled-cell predictor
   KK_COUNT
 };
 

@@ -623,6 +623,12 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     k_finalize_dt<<<1, 1, 0, s>>>(h->sc, h->cfl_h, cfg.use_fixed_dt, cfg.fixed_dt, c.first_stage, c.has_target,
                                   c.t, c.target);
   }
+  // learned predictor: flags from W and the extrema just reduced
+  const uint8_t* pred = nullptr;
+  if (h->mlp && apost) {
+    if ((st = mlp_predict_stage(h, s))) return st;
+    pred = h->pred;
+  }
   const f2::V2<Tc> F = f2::make_v2((Tc*)h->F[ax[0]], g.nx + 1, g.ny, 0);
   const f2::V2<Tc> G = f2::make_v2((Tc*)h->F[ax[1]], g.nx, g.ny + 1, 0);
   // 2. fluxes (+ candidate)
@@ -635,7 +641,7 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     LaunchScope scope(KK_FACE, cells * 5 * (3.0 * sizeof(Tc) + (apost ? 16.0 : 0.0)), s);
     f2::V2<const Tc> Wc{(const Tc*)h->W, h->gW, g.ny + 2 * h->gW, (g.nx + 2 * h->gW) * (g.ny + 2 * h->gW)};
     kern<<<grid, 256, smem, s>>>(Wc, c.stage_in, g, F, G, apost ? h->Us : nullptr, crule, trule, lrule, rrule, ph,
-                                 cx, cy, h->sc);
+                                 cx, cy, h->sc, pred, 1, cfg.slope_limiter);
   }
   if ((st = set_cuda_error(h, "fused fluxes"))) return st;
   // 3. W* + detection
@@ -662,6 +668,7 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     kern<<<grid, 256, smem, s>>>(h->Us, g, Wc, crule, trule, ph, ds, h->sc, h->trouble, h->logs[0], h->logs[1],
                                  h->logs[2]);
     if ((st = set_cuda_error(h, "fused detect"))) return st;
+    if (pred && (st = mlp_count_stage(h, s))) return st;
   }
   // 4. fallback + divergence + Runge-Kutta
   {
@@ -681,15 +688,16 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     LaunchScope scope(KK_FINAL, cells * (5 * 2.0 * sizeof(Tc) + arrays * 40.0 + (apost ? 41.0 : 0.0)), s);
     f2::V2<const Tc> Fc{F.p, 0, F.sx, F.vs};
     f2::V2<const Tc> Gc{G.p, 0, G.sx, G.vs};
-    kern<<<grid, 256, smem, s>>>(c.stage_in, g, Fc, Gc, h->trouble, apost ? 1 : 0, 1, cfg.slope_limiter, ph, cx, cy,
-                                 c.spec, h->sc);
+    kern<<<grid, 256, smem, s>>>(c.stage_in, g, Fc, Gc, h->trouble, pred, apost ? 1 : 0, 1, cfg.slope_limiter, ph,
+                                 cx, cy, c.spec, h->sc);
   }
   return set_cuda_error(h, "fused final");
 }
 
 template <typename Tc>
 int run_stage_any(fvh_handle* h, const StageCall& c, cudaStream_t s) {
-  if (h->cfg.kernel_path != FVH_PATH_GENERIC && fused2d_eligible(h)) {
+  h->last_stage_fused = h->cfg.kernel_path != FVH_PATH_GENERIC && fused2d_eligible(h);
+  if (h->last_stage_fused) {
     int p = 0;
     for (int a = 0; a < 3; ++a)
       if (h->active[a]) p = h->p[a];

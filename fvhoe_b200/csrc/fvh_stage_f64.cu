@@ -11,7 +11,13 @@ __global__ void k_reset_scalars(Scalars* sc, int reset_step) {
   if (t == 0) {
     sc->cfl_key = 0ull;
     sc->troubled = 0u;
-    if (reset_step) sc->nonfinite = 0u;
+    if (reset_step) {
+      sc->nonfinite = 0u;
+      sc->predicted = 0u;
+      sc->judged = 0u;
+      sc->missed = 0u;
+      sc->false_alarm = 0u;
+    }
   }
   for (int v = t; v < kMaxVars; v += blockDim.x) {
     sc->vmax_key[v] = 0ull;

@@ -259,6 +259,51 @@ class EulerSolver(ODE):
         with torch.cuda.device(self.am("u").device):
             c.check(c.lib.fvh_create(ctypes.byref(self._cfg), ctypes.byref(handle)))
         self._handle = handle
+        self._predictor = None
+        self.pred_totals = None
+
+    # -- learned troubled-cell predictor (no counterpart in the reference) ------
+    def set_predictor(self, predictor, threshold: float = 0.5):
+        """Attaches a TroubledCellPredictor (None detaches). Needs the fused 2D
+        path, a-posteriori limiting and global NAD. Faces next to predicted
+        cells take the fallback flux; the a-posteriori check still runs on every
+        cell and revises the faces of cells the network missed."""
+        m = predictor._m if predictor is not None else None
+        self._capi.check(self._capi.lib.fvh_set_predictor(self._handle, m, float(threshold)), self._handle)
+        self._predictor = predictor
+        self.pred_totals = dict(predicted=0, troubled=0, missed=0, false_alarm=0, cell_stages=0)
+
+    def _count_predictions(self, stages):
+        if self._predictor is None:
+            return
+        st = self._capi.FvhPredStats()
+        self._capi.check(self._capi.lib.fvh_get_pred_stats(self._handle, ctypes.byref(st), self._stream()),
+                         self._handle)
+        for k in ("predicted", "troubled", "missed", "false_alarm"):
+            self.pred_totals[k] += int(getattr(st, k))
+        self.pred_totals["cell_stages"] += stages * int(np.prod(self.n))
+
+    def predictor_rates(self) -> dict:
+        """Miss rate (missed / troubled) and false-alarm rate (false alarms /
+        untroubled) accumulated over every stage since set_predictor."""
+        t = dict(self.pred_totals or {})
+        if not t:
+            return t
+        untroubled = t["cell_stages"] - t["troubled"]
+        t["miss_rate"] = t["missed"] / t["troubled"] if t["troubled"] else 0.0
+        t["false_alarm_rate"] = t["false_alarm"] / untroubled if untroubled else 0.0
+        return t
+
+    def predicted_flags(self) -> np.ndarray:
+        """Predicted flags (uint8, (nx, ny, nz)) of the last stage."""
+        import torch
+
+        out = torch.empty(self.n, dtype=torch.uint8, device=self.am("u").device)
+        self._capi.check(
+            self._capi.lib.fvh_pred_flags(self._handle, ctypes.c_void_p(out.data_ptr()), self._stream()),
+            self._handle,
+        )
+        return out.cpu().numpy()
 
     def _init_array_allocation(self):
         import torch
@@ -312,6 +357,7 @@ class EulerSolver(ODE):
         )
         if self._log_enabled:
             self.trouble_counter += 1
+        self._count_predictions(1)
         return dt.value, dudt
 
     def hydrodynamics(self, u):
@@ -333,6 +379,7 @@ class EulerSolver(ODE):
         self.f_evaluation_count += _STAGES[integrator]
         if self._log_enabled:
             self.trouble_counter += _STAGES[integrator]
+        self._count_predictions(_STAGES[integrator])
         return dt.value
 
     def step_helper_function(self):

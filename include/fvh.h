@@ -202,7 +202,8 @@ int fvh_get_stats(fvh_handle* h, fvh_stats* out, void* stream);
 #define FVH_KK_FALLBACK 5   /* MUSCL fallback + blend */
 #define FVH_KK_FINAL 6      /* flux divergence + Runge-Kutta combination */
 #define FVH_KK_SMALL 7      /* stage scalars, convex weights, log arithmetic */
-#define FVH_KK_COUNT 8
+#define FVH_KK_PREDICT 8    /* learned troubled-cell predictor (inference) */
+#define FVH_KK_COUNT 9
 
 /* Total kernel launches issued by this library in this process. */
 uint64_t fvh_kernel_launches(void);
@@ -216,6 +217,84 @@ int fvh_profile_enable(fvh_handle* h, int on);
  * move (inputs read once, outputs written once) and the launch counts
  * accumulated since the previous read, and clears them. */
 int fvh_profile_read(fvh_handle* h, double* ms, double* bytes, uint64_t* launches, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Learned troubled-cell predictor (no counterpart in the reference, whose
+ * troubled cells come only from the a-posteriori check,
+ * fvhoe/solver.py:653-732). A 100 -> 64 -> 64 -> 1 GELU network over the 5x5
+ * neighbourhood of (rho, v_X, v_Y, P) of each cell of a 2D grid, run on the
+ * tensor cores (BF16 operands, FP32 accumulation). Attached to a handle, it
+ * runs on the stage's primitives before the high-order fluxes; faces next to
+ * a predicted cell take the MUSCL fallback flux in the flux pass, the
+ * a-posteriori check still runs on every cell and the final pass revises the
+ * faces of troubled cells the network missed. The update is then the
+ * reference's with the fallback applied on (troubled | predicted) cells.
+ * Features: for each variable and offset (a, b) in [-2, 2]^2,
+ * d = w(x+a, y+b) - w(x, y), f = sign(d) log1p(|d| / (1e-5 R)) / log1p(1e5),
+ * R = the variable's range over the stage (the global NAD extrema), stored as
+ * 112 BF16 values per row (12 zero columns). Parameters: FP32, W1[64][100],
+ * b1[64], W2[64][64], b2[64], w3[64], b3 (both matrices output-major).
+ * ------------------------------------------------------------------------ */
+typedef struct fvh_mlp fvh_mlp;
+
+#define FVH_MLP_FEATURES 100
+#define FVH_MLP_ROW 112 /* BF16 values per stored feature row */
+
+/* Number of FP32 parameters (10689). */
+size_t fvh_mlp_param_count(void);
+
+/* Creates a network on a device with seeded He-normal weights, zero biases. */
+int fvh_mlp_create(int device, uint64_t seed, fvh_mlp** out);
+int fvh_mlp_destroy(fvh_mlp* m);
+/* Message of the last failure on m (or of fvh_mlp_create when m is NULL). */
+const char* fvh_mlp_last_error(const fvh_mlp* m);
+
+/* Host copies of the FP32 parameters; set also resets the Adam moments. */
+int fvh_mlp_get_params(fvh_mlp* m, float* host, size_t n);
+int fvh_mlp_set_params(fvh_mlp* m, const float* host, size_t n);
+
+/* Training rows from a handle's last stage (fused 2D path, a-posteriori with
+ * global NAD): X (device, nx*ny rows of FVH_MLP_ROW BF16 bit patterns) and
+ * the a-posteriori flags y (device, nx*ny bytes), row-major over (x, y). */
+int fvh_mlp_features(fvh_handle* h, uint16_t* X, uint8_t* y, void* stream);
+
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) on the mean binary cross-entropy
+ * with logits over n device rows, positives weighted by pos_weight;
+ * loss_out (host, may be NULL) receives the batch mean loss before the
+ * update and synchronises the stream. */
+int fvh_mlp_train_step(fvh_mlp* m, const uint16_t* X, const uint8_t* y, int n, float lr, float pos_weight,
+                       float* loss_out, void* stream);
+
+/* Gradients of that loss (device array of fvh_mlp_param_count() floats) and
+ * the loss (host, may be NULL; synchronises), without an update. */
+int fvh_mlp_gradients(fvh_mlp* m, const uint16_t* X, const uint8_t* y, int n, float pos_weight, float* grads_out,
+                      float* loss_out, void* stream);
+
+/* Logits of n device rows into the device array logits. */
+int fvh_mlp_logits(fvh_mlp* m, const uint16_t* X, int n, float* logits, void* stream);
+
+/* Tensor-core completion waits that reached their bound (0 when healthy). */
+unsigned int fvh_mlp_errors(fvh_mlp* m);
+
+/* Attaches m to h (NULL detaches); cells whose predicted probability exceeds
+ * threshold are flagged. Needs the fused 2D path, a-posteriori limiting with
+ * global NAD and a network on h's device; m must outlive the attachment. */
+int fvh_set_predictor(fvh_handle* h, fvh_mlp* m, float threshold);
+
+/* Predictor counts of the last step, summed over its stages. */
+typedef struct fvh_pred_stats {
+  unsigned int predicted;   /* cells the network flagged */
+  unsigned int troubled;    /* cells the a-posteriori check flagged */
+  unsigned int missed;      /* troubled, not predicted */
+  unsigned int false_alarm; /* predicted, not troubled */
+} fvh_pred_stats;
+
+/* Synchronises the stream. */
+int fvh_get_pred_stats(fvh_handle* h, fvh_pred_stats* out, void* stream);
+
+/* Copies the predicted flags of the last stage (uint8, nx*ny*nz) to the device
+ * array flags. */
+int fvh_pred_flags(fvh_handle* h, uint8_t* flags, void* stream);
 
 #ifdef __cplusplus
 }

@@ -752,11 +752,14 @@ def _convex_faces(trouble, cfg, tx, ty, tz):
 # ---------------------------------------------------------------------------
 # one RHS evaluation (fvhoe/solver.py:422-454, 653-732)
 # ---------------------------------------------------------------------------
-def rhs(u: np.ndarray, cfg: OracleConfig):
+def rhs(u: np.ndarray, cfg: OracleConfig, predicted: Optional[np.ndarray] = None):
     """(dt, dudt, info) for one stage.
 
     info holds the high-order fluxes, the candidate, the detector outputs and
     the face weights when a-posteriori limiting is on (fvhoe/solver.py:429-454).
+    `predicted` (bool, (nx, ny, nz)) adds cells whose faces take the fallback
+    flux whatever the check says: the learned predictor's mode, which has no
+    counterpart in the reference; the detector outputs stay the check's.
     """
     dt, fluxes = hydrofluxes(u, cfg, cfg.p)
     info = {"dt": dt}
@@ -770,10 +773,11 @@ def rhs(u: np.ndarray, cfg: OracleConfig):
         if cfg.force_trouble:
             trouble = np.ones_like(trouble, dtype=bool)
         info.update(ustar=ustar, trouble=trouble, nad_mag=nad_mag, pad_mag=pad_mag)
-        if np.any(trouble):
+        blend = trouble if predicted is None else (trouble | np.asarray(predicted, dtype=bool))
+        if np.any(blend):
             p_fb = tuple(int(cfg.p[a] > 0) for a in range(3))
             _, low = hydrofluxes(u, cfg, p_fb, limiter=cfg.slope_limiter)
-            thetas = face_trouble(trouble, cfg)
+            thetas = face_trouble(blend, cfg)
             for d in range(3):
                 if act[d]:
                     fluxes[d] = (1 - thetas[d]) * fluxes[d] + thetas[d] * low[d]

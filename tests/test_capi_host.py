@@ -36,15 +36,35 @@ def test_config_struct_layout_matches_header(tmp_path):
 
     src = tmp_path / "size.c"
     src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "fvh.h"\n'
-                   'int main(){printf("%zu %zu %zu %zu\\n", sizeof(fvh_config), offsetof(fvh_config, device),'
-                   ' offsetof(fvh_config, pad_hi), sizeof(fvh_stats));return 0;}\n')
+                   'int main(){printf("%zu %zu %zu %zu %zu %d %d %d\\n", sizeof(fvh_config),'
+                   ' offsetof(fvh_config, device), offsetof(fvh_config, pad_hi), sizeof(fvh_stats),'
+                   ' sizeof(fvh_pred_stats), FVH_KK_COUNT, FVH_MLP_FEATURES, FVH_MLP_ROW);return 0;}\n')
     exe = tmp_path / "size"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
-    size, dev, pad_hi, stats = map(int, subprocess.run([str(exe)], capture_output=True, text=True).stdout.split())
+    out = subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()
+    size, dev, pad_hi, stats, pstats, kinds, feats, row = map(int, out)
     assert size == ctypes.sizeof(_capi.FvhConfig)
     assert dev == _capi.FvhConfig.device.offset
     assert pad_hi == _capi.FvhConfig.pad_hi.offset
     assert stats == ctypes.sizeof(_capi.FvhStats)
+    assert pstats == ctypes.sizeof(_capi.FvhPredStats)
+    assert kinds == len(_capi.KERNEL_KINDS)
+    assert (feats, row) == (_capi.MLP_FEATURES, _capi.MLP_ROW)
+
+
+def test_predictor_entry_points_refuse_null_arguments():
+    from fvhoe_b200 import _capi
+    from oracle import mlp_oracle
+
+    assert _capi.lib.fvh_mlp_param_count() == mlp_oracle.N_PARAMS
+    assert _capi.lib.fvh_mlp_create(0, 0, None) == _capi.ERR_ARG
+    assert _capi.lib.fvh_mlp_destroy(None) == _capi.OK
+    assert _capi.lib.fvh_mlp_get_params(None, None, 0) == _capi.ERR_ARG
+    assert _capi.lib.fvh_mlp_train_step(None, None, None, 0, 0.0, 1.0, None, None) == _capi.ERR_ARG
+    assert _capi.lib.fvh_mlp_logits(None, None, 0, None, None) == _capi.ERR_ARG
+    assert _capi.lib.fvh_set_predictor(None, None, 0.5) == _capi.ERR_ARG
+    assert _capi.lib.fvh_get_pred_stats(None, None, None) == _capi.ERR_ARG
+    assert _capi.lib.fvh_pred_flags(None, None, None) == _capi.ERR_ARG
 
 
 def test_default_config_matches_reference_defaults():
