@@ -527,7 +527,10 @@ def run_ours(args):
         if world == 1 and not args.no_predictor:
             del chosen
             torch.cuda.empty_cache()
-            line["learned_predictor"] = predictor_leg(args, stream, sp)
+            try:
+                line["learned_predictor"] = predictor_leg(args, stream, sp)
+            except Exception as exc:  # the headline line is printed whatever this leg does
+                line["learned_predictor"] = {"error": f"{type(exc).__name__}: {exc}"}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -535,6 +538,9 @@ def run_ours(args):
 
 
 def main():
+    import faulthandler
+
+    faulthandler.enable()
     args = parse()
     if args.impl == "reference":
         run_reference(args)

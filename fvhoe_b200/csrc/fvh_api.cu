@@ -35,16 +35,18 @@ void Profiler::record_begin(int kind, double bytes, cudaStream_t s) {
   p.kind = kind;
   p.bytes = bytes;
   cudaEventRecord(p.a, s);
+  open_.push_back(used_.size());
   used_.push_back(p);
-  open_ = &used_.back();
 }
 
 void Profiler::record_end(cudaStream_t s) {
-  if (open_) cudaEventRecord(open_->b, s);
-  open_ = nullptr;
+  if (open_.empty()) return;
+  cudaEventRecord(used_[open_.back()].b, s);
+  open_.pop_back();
 }
 
 int Profiler::collect(KernelTotals& t) {
+  if (!open_.empty()) return FVH_ERR_CUDA;  // a scope is still open
   for (auto& p : used_) {
     if (cudaEventSynchronize(p.b) != cudaSuccess) return FVH_ERR_CUDA;
     float ms = 0.f;

@@ -33,7 +33,8 @@ namespace {
 
 thread_local std::string g_mlp_error;
 
-constexpr int kPredictSmem = kRows * kInPad * 2 + kRows * kHidden * 2 + kImgB1 + kImgB2 + 256 * 4;
+// inference tile: features (the first layer's operand, then the second's), images, FP32 vectors
+constexpr int kPredictSmem = kRows * kInPad * 2 + kImgB1 + kImgB2 + 256 * 4;
 
 // Training tile layout (bytes of dynamic shared memory). Operands of the
 // forward GEMMs (rows = samples), of dh1 = dz2 W2, and of the weight-gradient
@@ -138,14 +139,16 @@ __device__ __forceinline__ void block_tmem_release(uint32_t tmem_base, uint32_t 
 // stage's FV primitives W (2D view with g ghosts).
 // ---------------------------------------------------------------------------
 template <typename Tw>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 4)
     k_mlp_predict(const Tw* __restrict__ W, int g, int nx, int ny, int4 vid4, const Scalars* __restrict__ sc,
                   const unsigned char* __restrict__ img, const float* __restrict__ params, float thr_logit,
                   uint8_t* __restrict__ pred, unsigned int* __restrict__ err) {
   extern __shared__ __align__(128) unsigned char sm[];
   unsigned char* A = sm;
-  unsigned char* A2 = A + kRows * kInPad * 2;
-  unsigned char* B1 = A2 + kRows * kHidden * 2;
+  // h1 reuses the feature tile: the first GEMM has completed when it is written,
+  // and the second has completed before the next tile's features are
+  unsigned char* A2 = A;
+  unsigned char* B1 = A + kRows * kInPad * 2;
   unsigned char* B2 = B1 + kImgB1;
   float* pb = reinterpret_cast<float*>(B2 + kImgB2);  // b1, b2, w3, b3
   __shared__ uint64_t bar;
@@ -170,30 +173,41 @@ __global__ void __launch_bounds__(128)
   const int vs = (nx + 2 * g) * sx;
   const int ncell = nx * ny;
   const int r = threadIdx.x;
+  const uint32_t lane = (uint32_t)(threadIdx.x & ~31) << 16;
   uint32_t phase = 0;
   for (int tile = blockIdx.x; tile * kRows < ncell; tile += gridDim.x) {
     const int cell = tile * kRows + r;
     const bool valid = cell < ncell;
-    float f[kIn];
+    // features straight into the operand tile, one 16-byte row of a core matrix per chunk
     if (valid) {
       const int x = cell / ny, y = cell - (cell / ny) * ny;
-      cell_features(W, sx, vs, (x + g) * sx + (y + g), vid, inv_s, f);
+      feature_row<Tw>(W, sx, vs, (x + g) * sx + (y + g), vid, inv_s, [&](int c, uint4 q) {
+        *reinterpret_cast<uint4*>(A + tc::kmajor_offset(r, 8 * c, kRows)) = q;
+      });
     } else {
 #pragma unroll
-      for (int k = 0; k < kIn; ++k) f[k] = 0.0f;
+      for (int c = 0; c < kInPad / 8; ++c)
+        *reinterpret_cast<uint4*>(A + tc::kmajor_offset(r, 8 * c, kRows)) = make_uint4(0u, 0u, 0u, 0u);
     }
-#pragma unroll
-    for (int k = 0; k < kInPad; ++k) store_bf16(A, tc::kmajor_offset(r, k, kRows), k < kIn ? f[k] : 0.0f);
     if (!run_gemm(tb, A, B1, kInPad, kHidden, &bar, phase, err)) break;
-    float h[kHidden];
-    load_row64(tb, 0, h);
 #pragma unroll
-    for (int j = 0; j < kHidden; ++j) store_bf16(A2, tc::kmajor_offset(r, j, kRows), gelu(h[j] + pb[j]));
+    for (int c = 0; c < kHidden / 16; ++c) {
+      float h[16];
+      tc::tmem_ld16(tb + lane + (uint32_t)(16 * c), h);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) h[j] = gelu(h[j] + pb[16 * c + j]);
+      *reinterpret_cast<uint4*>(A2 + tc::kmajor_offset(r, 16 * c, kRows)) = pack_bf16x8(h);
+      *reinterpret_cast<uint4*>(A2 + tc::kmajor_offset(r, 16 * c + 8, kRows)) = pack_bf16x8(h + 8);
+    }
     if (!run_gemm(tb + 64, A2, B2, kHidden, kHidden, &bar, phase, err)) break;
-    load_row64(tb, 64, h);
     float logit = pb[192];
 #pragma unroll
-    for (int j = 0; j < kHidden; ++j) logit += gelu(h[j] + pb[64 + j]) * pb[128 + j];
+    for (int c = 0; c < kHidden / 16; ++c) {
+      float h[16];
+      tc::tmem_ld16(tb + lane + (uint32_t)(64 + 16 * c), h);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) logit = fmaf(gelu(h[j] + pb[64 + 16 * c + j]), pb[128 + 16 * c + j], logit);
+    }
     if (valid) pred[cell] = logit > thr_logit ? 1 : 0;
     tc::fence_before_sync();
     __syncthreads();
@@ -418,11 +432,8 @@ __global__ void k_mlp_features(const Tw* __restrict__ W, int g, int nx, int ny, 
   const int vs = (nx + 2 * g) * sx;
   for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < nx * ny; cell += gridDim.x * blockDim.x) {
     const int x = cell / ny, yy = cell - (cell / ny) * ny;
-    float f[kIn];
-    cell_features(W, sx, vs, (x + g) * sx + (yy + g), vid, inv_s, f);
-    __nv_bfloat16* row = X + (size_t)cell * kInPad;
-#pragma unroll
-    for (int k = 0; k < kInPad; ++k) row[k] = __float2bfloat16_rn(k < kIn ? f[k] : 0.0f);
+    uint4* row = reinterpret_cast<uint4*>(X + (size_t)cell * kInPad);
+    feature_row<Tw>(W, sx, vs, (x + g) * sx + (yy + g), vid, inv_s, [&](int c, uint4 q) { row[c] = q; });
     y[cell] = trouble[cell];
   }
 }
@@ -484,7 +495,7 @@ int mlp_predict_stage(fvh_handle* h, cudaStream_t s) {
   const int nx = h->n[ax[0]], ny = h->n[ax[1]];
   const int4 vid = make_int4(0, 1 + ax[0], 1 + ax[1], 4);
   const int tiles = (nx * ny + kRows - 1) / kRows;
-  const int grid = tiles < 148 * 3 ? tiles : 148 * 3;
+  const int grid = tiles < 148 * 4 ? tiles : 148 * 4;  // 4 CTAs per SM: shared memory and TMEM both allow it
   LaunchScope scope(KK_PREDICT, (double)nx * ny * (4 * h->elem + 1), s);
   if (h->elem == sizeof(float)) {
     cudaFuncSetAttribute(k_mlp_predict<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPredictSmem);

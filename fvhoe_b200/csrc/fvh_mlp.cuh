@@ -1,5 +1,6 @@
-// Learned troubled-cell predictor: a 100 -> 64 -> 64 -> 1 GELU network over
-// the 5x5 neighbourhood of (rho, v_X, v_Y, P) around each cell of a 2D grid.
+// Learned troubled-cell predictor: a 100 -> 64 -> 64 -> 1 network with GELU
+// (tanh form) activations over the 5x5 neighbourhood of (rho, v_X, v_Y, P)
+// around each cell of a 2D grid.
 //
 // Features (computed from the stage's FV primitives W): for each variable v
 // and offset (a, b) in [-2, 2]^2, d = W_v(x+a, y+b) - W_v(x, y) and
@@ -43,11 +44,24 @@ constexpr int kImgB2 = kHidden * kHidden * 2;   // W2 as N = j x K = i (forward)
 constexpr int kImgB2t = kHidden * kHidden * 2;  // W2 as N = i x K = j (backward)
 constexpr int kImgBytes = kImgB1 + kImgB2 + kImgB2t;
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+// GELU in its tanh form, 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3)))
+// (Hendrycks & Gimpel, "Gaussian Error Linear Units", 2016), with the
+// hardware tanh approximation (tanh.approx.f32, absolute error near 2^-11,
+// below the BF16 rounding of the activations).
+__device__ __forceinline__ float tanh_approx(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+constexpr float kGeluC = 0.7978845608028654f;  // sqrt(2 / pi)
+constexpr float kGeluA = 0.044715f;
+__device__ __forceinline__ float gelu(float x) {
+  const float t = tanh_approx(kGeluC * fmaf(kGeluA * x, x * x, x));
+  return 0.5f * x * (1.0f + t);
+}
 __device__ __forceinline__ float gelu_grad(float x) {
-  const float cdf = 0.5f * (1.0f + erff(x * 0.70710678118654752f));
-  const float pdf = 0.39894228040143268f * __expf(-0.5f * x * x);
-  return cdf + x * pdf;
+  const float t = tanh_approx(kGeluC * fmaf(kGeluA * x, x * x, x));
+  return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * kGeluC * fmaf(3.0f * kGeluA, x * x, 1.0f);
 }
 
 __device__ __forceinline__ void store_bf16(unsigned char* tile, uint32_t off, float v) {
@@ -56,26 +70,51 @@ __device__ __forceinline__ void store_bf16(unsigned char* tile, uint32_t off, fl
 __device__ __forceinline__ float load_bf16(const unsigned char* tile, uint32_t off) {
   return __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(tile + off));
 }
+// Eight floats as eight BF16 values (round to nearest even), first at the lowest address.
+__device__ __forceinline__ uint4 pack_bf16x8(const float* v) {
+  uint4 q;
+  uint32_t* w = reinterpret_cast<uint32_t*>(&q);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+    w[i] = *reinterpret_cast<const uint32_t*>(&h);
+  }
+  return q;
+}
 
-// Feature vector of the cell at offset o of a 2D primitive array (row stride
-// sx, variable stride vs); vid = primitive indices of (rho, v_X, v_Y, P),
-// inv_s[v] = 1 / (eps R_v).
-template <typename Tw>
-__device__ __forceinline__ void cell_features(const Tw* __restrict__ W, int sx, int vs, int o, const int* vid,
-                                              const float* inv_s, float* f) {
-  const float norm = 1.0f / log1pf(1.0f / kEps);
+// Features [8 C, 8 C + 8) of the cell at offset o of a 2D primitive array (row
+// stride sx, variable stride vs), packed as BF16; vid = primitive indices of
+// (rho, v_X, v_Y, P), inv_s[v] = 1 / (eps R_v). Feature k = v*25 + (a+2)*5 +
+// (b+2) is sign(d) ln(1 + |d| inv_s) / ln(1 + 1/eps) with d = w(x+a, y+b) -
+// w(x, y) taken in the precision of W; k >= 100 is zero.
+template <typename Tw, int C>
+__device__ __forceinline__ uint4 feature_chunk(const Tw* __restrict__ W, int sx, int vs, int o, const int* vid,
+                                               const float* inv_s) {
+  constexpr float kNorm = 0.08685882093641431f;  // 1 / ln(1 + 1e5)
+  float f[8];
 #pragma unroll
-  for (int v = 0; v < 4; ++v) {
+  for (int i = 0; i < 8; ++i) {
+    const int k = 8 * C + i;
+    if (k >= kIn) {
+      f[i] = 0.0f;
+      continue;
+    }
+    const int v = k / 25, a = (k % 25) / 5 - 2, b = (k % 5) - 2;
     const Tw* base = W + vid[v] * vs + o;
-    const Tw c = base[0];
-#pragma unroll
-    for (int a = -2; a <= 2; ++a)
-#pragma unroll
-      for (int b = -2; b <= 2; ++b) {
-        const float d = (float)(base[a * sx + b] - c);  // difference in the precision of W
-        const float m = log1pf(fabsf(d) * inv_s[v]) * norm;
-        f[v * 25 + (a + 2) * 5 + (b + 2)] = d < 0.0f ? -m : m;
-      }
+    const float d = (float)(base[a * sx + b] - base[0]);
+    const float m = __logf(fmaf(fabsf(d), inv_s[v], 1.0f)) * kNorm;
+    f[i] = d < 0.0f ? -m : m;
+  }
+  return pack_bf16x8(f);
+}
+
+// All 14 chunks of a cell's feature row, handed to store(c, chunk).
+template <typename Tw, int C = 0, typename Store>
+__device__ __forceinline__ void feature_row(const Tw* __restrict__ W, int sx, int vs, int o, const int* vid,
+                                            const float* inv_s, Store&& store) {
+  if constexpr (C < kInPad / 8) {
+    store(C, feature_chunk<Tw, C>(W, sx, vs, o, vid, inv_s));
+    feature_row<Tw, C + 1>(W, sx, vs, o, vid, inv_s, store);
   }
 }
 

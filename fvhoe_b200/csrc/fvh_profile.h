@@ -50,7 +50,7 @@ class Profiler {
   };
   std::vector<Pair> used_;
   std::vector<Pair> pool_;
-  Pair* open_ = nullptr;
+  std::vector<size_t> open_;  // indices into used_ of the scopes still open (nested scopes allowed)
 };
 
 // Profiler of the calling thread (nullptr when profiling is off).

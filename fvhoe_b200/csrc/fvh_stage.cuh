@@ -668,8 +668,8 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     kern<<<grid, 256, smem, s>>>(h->Us, g, Wc, crule, trule, ph, ds, h->sc, h->trouble, h->logs[0], h->logs[1],
                                  h->logs[2]);
     if ((st = set_cuda_error(h, "fused detect"))) return st;
-    if (pred && (st = mlp_count_stage(h, s))) return st;
   }
+  if (pred && (st = mlp_count_stage(h, s))) return st;
   // 4. fallback + divergence + Runge-Kutta
   {
     using D = f2::FinalDims<T::EX, T::EY>;

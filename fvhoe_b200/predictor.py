@@ -16,6 +16,7 @@ faces of the cells the network missed.
 """
 
 import ctypes
+import sys
 from typing import Iterable, Optional, Tuple
 
 import numpy as np
@@ -53,7 +54,8 @@ class TroubledCellPredictor:
 
     def __del__(self):
         m = getattr(self, "_m", None)
-        if m:
+        # at interpreter exit the CUDA runtime may already be torn down; the process frees everything
+        if m and not sys.is_finalizing():
             _capi.lib.fvh_mlp_destroy(m)
             self._m = None
 

@@ -18,6 +18,7 @@ import json
 import os
 import pickle
 import shutil
+import sys
 from typing import Callable, Dict, Iterable, Tuple
 
 import numpy as np
@@ -314,7 +315,8 @@ class EulerSolver(ODE):
 
     def __del__(self):
         handle = getattr(self, "_handle", None)
-        if handle is not None and handle.value:
+        # at interpreter exit the CUDA runtime may already be torn down; the process frees everything
+        if handle is not None and handle.value and not sys.is_finalizing():
             try:
                 self._capi.lib.fvh_destroy(handle)
             except Exception:

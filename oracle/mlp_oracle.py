@@ -9,7 +9,7 @@ this module is the CPU definition the CUDA kernels are checked against:
   f = sign(d) log1p(|d| / (eps R)) / log1p(1 / eps), eps = 1e-5, with R the
   variable's range over the stage's 3-ghost box (the global NAD extrema of
   `fvhoe/slope_limiting.py:118-140`);
-* network 100 -> 64 -> 64 -> 1 with exact (erf) GELU, parameters packed as
+* network 100 -> 64 -> 64 -> 1 with GELU in its tanh form, parameters packed as
   W1[64][100], b1, W2[64][64], b2, w3[64], b3 (FP32);
 * loss: binary cross-entropy with logits, positives weighted by pos_weight,
   averaged over the batch.
@@ -81,15 +81,18 @@ def features(w, vid, ranges, ghosts):
     return out.reshape(nx * ny, N_IN)
 
 
-_erf = np.vectorize(math.erf)
+_C = math.sqrt(2.0 / math.pi)
+_A = 0.044715
 
 
 def _gelu(x):
-    return 0.5 * x * (1.0 + _erf(x / math.sqrt(2.0)))
+    """GELU, tanh form (Hendrycks & Gimpel 2016)."""
+    return 0.5 * x * (1.0 + np.tanh(_C * (x + _A * x ** 3)))
 
 
 def _gelu_grad(x):
-    return 0.5 * (1.0 + _erf(x / math.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / math.sqrt(2.0 * math.pi)
+    t = np.tanh(_C * (x + _A * x ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * _C * (1.0 + 3.0 * _A * x * x)
 
 
 def _round(x, on):
