@@ -177,15 +177,19 @@ def hbm_peak():
 
 
 def ncu_traffic(kind, n, p, precision):
-    """DRAM bytes per launch of `kind` from the committed ncu summary, scaled to n^2 cells."""
-    path = os.path.join(ROOT, "profiles", "traffic_kh_per_launch.json")
-    try:
+    """DRAM bytes per launch of `kind` from the committed ncu summaries (lines
+    `traffic <precision>_p<p> <kind> cells=C bytes=B`), scaled to n^2 cells."""
+    import glob
+
+    key = f"{precision}_p{p}"
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
         with open(path) as fh:
-            data = json.load(fh)
-        rec = data[f"{precision}_p{p}"][kind]
-        return rec["bytes_per_launch"] * (n * n) / rec["cells"]
-    except (OSError, KeyError, ValueError, TypeError):
-        return None
+            for line in fh:
+                f = line.split()
+                if len(f) == 5 and f[0] == "traffic" and f[1] == key and f[2] == kind:
+                    cells = int(f[3].split("=")[1])
+                    return int(f[4].split("=")[1]) * (n * n) / cells
+    return None
 
 
 # ---------------------------------------------------------------------------
