@@ -32,6 +32,7 @@ __all__ = [
     "ArrayManager",
     "BoundaryCondition",
     "DoubleShock1D",
+    "Ensemble",
     "EulerSolver",
     "FourQuadrant2D",
     "HydroState",
@@ -52,9 +53,13 @@ __all__ = [
 
 
 def __getattr__(name):
-    # the predictor module binds libfvh.so at import; load it on first use
+    # these modules bind libfvh.so at import; load them on first use
     if name in ("TroubledCellPredictor", "collect_training_data"):
         from . import predictor
 
         return getattr(predictor, name)
+    if name == "Ensemble":
+        from .ensemble import Ensemble
+
+        return Ensemble
     raise AttributeError(f"module {__name__!r} has no attribute {name!r}")

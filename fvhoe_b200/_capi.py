@@ -60,6 +60,20 @@ EXPORTS = (
     "fvh_set_predictor",
     "fvh_get_pred_stats",
     "fvh_pred_flags",
+    "fvh_ensemble_create",
+    "fvh_ensemble_destroy",
+    "fvh_ensemble_last_error",
+    "fvh_ensemble_bytes",
+    "fvh_ensemble_state",
+    "fvh_ensemble_load",
+    "fvh_ensemble_store",
+    "fvh_ensemble_reset",
+    "fvh_ensemble_step",
+    "fvh_ensemble_status",
+    "fvh_ensemble_configure",
+    "fvh_ensemble_variant_info",
+    "fvh_ensemble_autotune",
+    "fvh_ensemble_graph_info",
 )
 
 KERNEL_KINDS = ("centre", "transverse", "face", "candidate", "detect", "fallback", "final", "small", "predict")
@@ -181,6 +195,30 @@ def _load():
     lib.fvh_set_predictor.argtypes = [vp, vp, ctypes.c_float]
     lib.fvh_get_pred_stats.argtypes = [vp, ctypes.POINTER(FvhPredStats), vp]
     lib.fvh_pred_flags.argtypes = [vp, vp, vp]
+    ip = ctypes.POINTER(ctypes.c_int)
+    up = ctypes.POINTER(ctypes.c_uint)
+    lib.fvh_ensemble_create.argtypes = [ctypes.POINTER(FvhConfig), ctypes.c_int, ip, ip, dp, dp, ctypes.POINTER(vp)]
+    lib.fvh_ensemble_destroy.argtypes = [vp]
+    lib.fvh_ensemble_last_error.argtypes = [vp]
+    lib.fvh_ensemble_last_error.restype = ctypes.c_char_p
+    lib.fvh_ensemble_bytes.argtypes = [vp]
+    lib.fvh_ensemble_bytes.restype = ctypes.c_size_t
+    lib.fvh_ensemble_state.argtypes = [vp, ctypes.c_int]
+    lib.fvh_ensemble_state.restype = vp
+    lib.fvh_ensemble_load.argtypes = [vp, ctypes.c_int, vp, vp]
+    lib.fvh_ensemble_store.argtypes = [vp, ctypes.c_int, vp, vp]
+    lib.fvh_ensemble_reset.argtypes = [vp, ctypes.c_double, ctypes.c_double, vp]
+    lib.fvh_ensemble_step.argtypes = [vp, ctypes.c_int, vp]
+    lib.fvh_ensemble_status.argtypes = [vp, dp, ip, ip, up, vp]
+    lib.fvh_ensemble_configure.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.fvh_ensemble_variant_info.argtypes = [vp, ctypes.c_int, ip, ip, ip, ctypes.POINTER(ctypes.c_size_t)]
+    lib.fvh_ensemble_autotune.argtypes = [vp, ctypes.c_int, ip, ip, dp, vp]
+    lib.fvh_ensemble_graph_info.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_char_p)]
+    for name in ("fvh_ensemble_create", "fvh_ensemble_destroy", "fvh_ensemble_load", "fvh_ensemble_store",
+                 "fvh_ensemble_reset", "fvh_ensemble_step",
+                 "fvh_ensemble_status", "fvh_ensemble_configure", "fvh_ensemble_variant_info",
+                 "fvh_ensemble_autotune", "fvh_ensemble_graph_info"):
+        getattr(lib, name).restype = ctypes.c_int
     for name in ("fvh_create", "fvh_destroy", "fvh_rhs", "fvh_step", "fvh_primitives", "fvh_trouble_flags",
                  "fvh_trouble_log", "fvh_set_log_mode", "fvh_get_stats", "fvh_profile_enable", "fvh_profile_read",
                  "fvh_mlp_create", "fvh_mlp_destroy", "fvh_mlp_get_params", "fvh_mlp_set_params", "fvh_mlp_features",

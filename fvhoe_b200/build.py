@@ -35,6 +35,10 @@ UNITS = {
     "fvh_noalloc.cu": ["-fmad=false"],
     # learned troubled-cell predictor (tensor cores, FP32 epilogues)
     "fvh_mlp.cu": [],
+    # batched ensemble: host API and one launch unit per precision
+    "fvh_ensemble.cu": [],
+    "fvh_ens_f64.cu": ["-fmad=false"],
+    "fvh_ens_f32.cu": ["-fmad=true", "--use_fast_math"],
 }
 
 
@@ -65,12 +69,14 @@ def _compile(unit, flags, verbose):
     return obj, res.stderr
 
 
-def build(force: bool = False, jobs: int = 3, verbose: bool = False) -> str:
+def build(force: bool = False, jobs: int = 0, verbose: bool = False) -> str:
     """Compiles every unit for sm_100a and links libfvh.so; returns its path."""
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= _sources_mtime():
         return LIB
+    if jobs <= 0:
+        jobs = min(len(UNITS), os.cpu_count() or 1)
     with ThreadPoolExecutor(max_workers=max(1, jobs)) as ex:
         results = list(ex.map(lambda kv: _compile(kv[0], kv[1], verbose), UNITS.items()))
     if verbose:
@@ -89,7 +95,7 @@ def build(force: bool = False, jobs: int = 3, verbose: bool = False) -> str:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
-    ap.add_argument("-j", type=int, default=3)
+    ap.add_argument("-j", type=int, default=0, help="parallel nvcc jobs (0: one per unit, at most the CPU count)")
     ap.add_argument("-v", action="store_true", help="print ptxas resource usage")
     args = ap.parse_args()
     print(build(force=args.force, jobs=args.j, verbose=args.v))

@@ -44,7 +44,7 @@ struct V2 {
 };
 
 template <typename T>
-inline V2<T> make_v2(T* p, int nx, int ny, int g) {
+__host__ __device__ inline V2<T> make_v2(T* p, int nx, int ny, int g) {
   V2<T> v;
   v.p = p;
   v.g = g;
@@ -261,16 +261,18 @@ __device__ __forceinline__ void reduce_keys_and_publish(unsigned long long cfl_k
 // k2_primitives: W over [-gw_out, n+gw_out)^2 in tiles of TX x TY outputs,
 // with the CFL maximum and the per-variable extrema (REDUCE).
 // ---------------------------------------------------------------------------
+// Tile functions: the body of each kernel for the tile (bx, by) (bx along Y,
+// by along X), so that one-problem launches (one tile per block) and the
+// batched ensemble (blocks looping over the tiles of many problems) share it.
 template <typename Tc, int P, int TX, int TY, int KC, bool REDUCE>
-__global__ void __launch_bounds__(256)
-    k2_primitives(const double* __restrict__ u, Geo g, V2<Tc> W, int gw_out, Rule<Tc, KC> c, Rule<Tc, KC> t,
-                  Phys<Tc> ph, ReduceSpec rs, Scalars* __restrict__ sc) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void tile2_primitives(const double* __restrict__ u, Geo g, V2<Tc> W, int gw_out,
+                                                 Rule<Tc, KC> c, Rule<Tc, KC> t, Phys<Tc> ph, ReduceSpec rs,
+                                                 Scalars* __restrict__ sc, int bx, int by, unsigned char* smem_raw) {
   using D = PrimsDims<P, TX, TY>;
   Tc* A = reinterpret_cast<Tc*>(smem_raw);
   Tc* B = A + D::A;
-  const int x0 = -gw_out + blockIdx.y * TX;
-  const int y0 = -gw_out + blockIdx.x * TY;
+  const int x0 = -gw_out + by * TX;
+  const int y0 = -gw_out + bx * TY;
   primitives_tile<Tc, P, TX, TY, KC>(u, g, x0, y0, A, B, c, t, ph);
   unsigned long long cfl_key = 0ull, kmax[5], kmin[5];
 #pragma unroll
@@ -307,6 +309,14 @@ __global__ void __launch_bounds__(256)
   if constexpr (REDUCE) reduce_keys_and_publish(cfl_key, kmax, kmin, rs, sc);
 }
 
+template <typename Tc, int P, int TX, int TY, int KC, bool REDUCE>
+__global__ void __launch_bounds__(256)
+    k2_primitives(const double* __restrict__ u, Geo g, V2<Tc> W, int gw_out, Rule<Tc, KC> c, Rule<Tc, KC> t,
+                  Phys<Tc> ph, ReduceSpec rs, Scalars* __restrict__ sc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  tile2_primitives<Tc, P, TX, TY, KC, REDUCE>(u, g, W, gw_out, c, t, ph, rs, sc, blockIdx.x, blockIdx.y, smem_raw);
+}
+
 // ---------------------------------------------------------------------------
 // k2_fluxes: high-order X- and Y-face fluxes of a TX x TY cell tile, and the
 // candidate u* = u + dt L(F) of its cells.
@@ -333,11 +343,11 @@ struct FluxDims {
 };
 
 template <typename Tc, int P, int TX, int TY, int KC, int KF>
-__global__ void __launch_bounds__(256)
-    k2_fluxes(V2<const Tc> W, const double* __restrict__ u, Geo g, V2<Tc> F, V2<Tc> G, double* __restrict__ ustar,
-              Rule<Tc, KC> c, Rule<Tc, KC> t, Rule<Tc, KF> lrule, Rule<Tc, KF> rrule, Phys<Tc> ph, double cx,
-              double cy, const Scalars* __restrict__ sc, const uint8_t* __restrict__ pred, int muscl, int limiter) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __restrict__ u, Geo g, V2<Tc> F, V2<Tc> G,
+                                             double* __restrict__ ustar, Rule<Tc, KC> c, Rule<Tc, KC> t,
+                                             Rule<Tc, KF> lrule, Rule<Tc, KF> rrule, Phys<Tc> ph, double cx,
+                                             double cy, double dt, const uint8_t* __restrict__ pred, int muscl,
+                                             int limiter, int bx, int by, unsigned char* smem_raw) {
   using D = FluxDims<P, TX, TY>;
   constexpr int R = D::R, RC = D::RC, H = D::H;
   Tc* Ws = reinterpret_cast<Tc*>(smem_raw);
@@ -346,7 +356,7 @@ __global__ void __launch_bounds__(256)
   Tc* FX = B + D::SB;
   Tc* GY = FX + D::SF;
   const int nt = blockDim.x;
-  const int x0 = blockIdx.y * TX, y0 = blockIdx.x * TY;
+  const int x0 = by * TX, y0 = bx * TY;
   // W tile with H ghosts (W holds gW >= H ghosts)
   for (int i = threadIdx.x; i < D::WX * D::WY; i += nt) {
     const int r = i / D::WY, q = i - r * D::WY;
@@ -476,7 +486,6 @@ __global__ void __launch_bounds__(256)
   if (!ustar) return;
   __syncthreads();
   // candidate u* = u + dt (0 + cx (F[i+1]-F[i]) + cy (G[j+1]-G[j]))
-  const double dt = sc->dt_stage;
   const int plane = g.nx * g.ny;
   for (int i = threadIdx.x; i < TX * TY; i += nt) {
     const int r = i / TY, q = i - r * TY;
@@ -525,21 +534,31 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+template <typename Tc, int P, int TX, int TY, int KC, int KF>
+__global__ void __launch_bounds__(256)
+    k2_fluxes(V2<const Tc> W, const double* __restrict__ u, Geo g, V2<Tc> F, V2<Tc> G, double* __restrict__ ustar,
+              Rule<Tc, KC> c, Rule<Tc, KC> t, Rule<Tc, KF> lrule, Rule<Tc, KF> rrule, Phys<Tc> ph, double cx,
+              double cy, const Scalars* __restrict__ sc, const uint8_t* __restrict__ pred, int muscl, int limiter) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  tile2_fluxes<Tc, P, TX, TY, KC, KF>(W, u, g, F, G, ustar, c, t, lrule, rrule, ph, cx, cy, sc->dt_stage, pred, muscl,
+                                      limiter, blockIdx.x, blockIdx.y, smem_raw);
+}
+
 // ---------------------------------------------------------------------------
 // k2_detect: W* of u* on the tile and 3 ghosts, then the detection of the
 // tile's cells against W (global, >= 3 ghosts).
 // ---------------------------------------------------------------------------
 template <typename Tc, int P, int TX, int TY, int KC>
-__global__ void __launch_bounds__(256)
-    k2_detect(const double* __restrict__ ustar, Geo g, V2<const Tc> W, Rule<Tc, KC> c, Rule<Tc, KC> t, Phys<Tc> ph,
-              DetectSpec ds, Scalars* __restrict__ sc, uint8_t* __restrict__ trouble, double* __restrict__ log_trouble,
-              double* __restrict__ log_nad, double* __restrict__ log_pad) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void tile2_detect(const double* __restrict__ ustar, Geo g, V2<const Tc> W, Rule<Tc, KC> c,
+                                             Rule<Tc, KC> t, Phys<Tc> ph, DetectSpec ds, Scalars* __restrict__ sc,
+                                             uint8_t* __restrict__ trouble, double* __restrict__ log_trouble,
+                                             double* __restrict__ log_nad, double* __restrict__ log_pad, int bx,
+                                             int by, unsigned char* smem_raw) {
   constexpr int OX = TX + 6, OY = TY + 6;
   using D = PrimsDims<P, OX, OY>;
   Tc* A = reinterpret_cast<Tc*>(smem_raw);
   Tc* B = A + D::A;
-  const int x0 = blockIdx.y * TX, y0 = blockIdx.x * TY;
+  const int x0 = by * TX, y0 = bx * TY;
   primitives_tile<Tc, P, OX, OY, KC>(ustar, g, x0 - 3, y0 - 3, A, B, c, t, ph);
   // A now holds W* on [x0-3, x0+TX+3) x [y0-3, y0+TY+3)
   Tc grange[5], glower[5], gupper[5];
@@ -633,6 +652,16 @@ __global__ void __launch_bounds__(256)
   block_count_add(count, &sc->troubled);
 }
 
+template <typename Tc, int P, int TX, int TY, int KC>
+__global__ void __launch_bounds__(256)
+    k2_detect(const double* __restrict__ ustar, Geo g, V2<const Tc> W, Rule<Tc, KC> c, Rule<Tc, KC> t, Phys<Tc> ph,
+              DetectSpec ds, Scalars* __restrict__ sc, uint8_t* __restrict__ trouble, double* __restrict__ log_trouble,
+              double* __restrict__ log_nad, double* __restrict__ log_pad) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  tile2_detect<Tc, P, TX, TY, KC>(ustar, g, W, c, t, ph, ds, sc, trouble, log_trouble, log_nad, log_pad, blockIdx.x,
+                                  blockIdx.y, smem_raw);
+}
+
 // ---------------------------------------------------------------------------
 // k2_final: fallback fluxes at troubled faces of the tile (from pointwise
 // primitives of the stage input with 2 ghosts), the blend with the
@@ -647,17 +676,17 @@ struct FinalDims {
 };
 
 template <typename Tc, int TX, int TY>
-__global__ void __launch_bounds__(256)
-    k2_final(const double* __restrict__ stage_in, Geo g, V2<const Tc> F, V2<const Tc> G,
-             const uint8_t* __restrict__ trouble, const uint8_t* __restrict__ pred, int apost, int muscl, int limiter,
-             Phys<Tc> ph, double cx, double cy, StageSpec st, Scalars* __restrict__ sc) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void tile2_final(const double* __restrict__ stage_in, Geo g, V2<const Tc> F,
+                                            V2<const Tc> G, const uint8_t* __restrict__ trouble,
+                                            const uint8_t* __restrict__ pred, int apost, int muscl, int limiter,
+                                            Phys<Tc> ph, double cx, double cy, StageSpec st, double dt_step,
+                                            Scalars* __restrict__ sc, int bx, int by, unsigned char* smem_raw) {
   using D = FinalDims<TX, TY>;
   Tc* Pw = reinterpret_cast<Tc*>(smem_raw);
   Tc* FX = Pw + D::SP;
   Tc* GY = FX + D::SF;
   const int nt = blockDim.x;
-  const int x0 = blockIdx.y * TX, y0 = blockIdx.x * TY;
+  const int x0 = by * TX, y0 = bx * TY;
   // high-order fluxes of the tile's faces
   for (int i = threadIdx.x; i < (TX + 1) * TY; i += nt) {
     const int f = i / TY, q = i - f * TY;
@@ -716,7 +745,7 @@ __global__ void __launch_bounds__(256)
   }
   __syncthreads();
   // divergence and the Runge-Kutta combination
-  const double dt = st.integrator == INT_RHS ? 0.0 : sc->dt_step;
+  const double dt = st.integrator == INT_RHS ? 0.0 : dt_step;
   const int plane = g.nx * g.ny;
   unsigned int bad = 0;
   for (int i = threadIdx.x; i < TX * TY; i += nt) {
@@ -789,6 +818,16 @@ __global__ void __launch_bounds__(256)
     }
   }
   block_count_add(bad, &sc->nonfinite);
+}
+
+template <typename Tc, int TX, int TY>
+__global__ void __launch_bounds__(256)
+    k2_final(const double* __restrict__ stage_in, Geo g, V2<const Tc> F, V2<const Tc> G,
+             const uint8_t* __restrict__ trouble, const uint8_t* __restrict__ pred, int apost, int muscl, int limiter,
+             Phys<Tc> ph, double cx, double cy, StageSpec st, Scalars* __restrict__ sc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  tile2_final<Tc, TX, TY>(stage_in, g, F, G, trouble, pred, apost, muscl, limiter, ph, cx, cy, st,
+                          st.integrator == INT_RHS ? 0.0 : sc->dt_step, sc, blockIdx.x, blockIdx.y, smem_raw);
 }
 
 }  // namespace f2

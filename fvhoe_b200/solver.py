@@ -34,6 +34,35 @@ _VAR_INDEX = {"rho": 0, "vx": 1, "mx": 1, "vy": 2, "my": 2, "vz": 3, "mz": 3, "P
 _STAGES = {"euler": 1, "ssprk2": 2, "ssprk3": 3, "rk4": 4}
 
 
+def _ic_functions(w0, hs, w0_passives, conservative_ic, fv_ic, gamma, h, p):
+    """(w0, u0, u0_fv) callables of an initial condition, as EulerSolver.__init__
+    builds them (fvhoe/solver.py:354-399)."""
+    ic_func = w0.build_ic(hs, w0_passives)
+    if not {"x", "y", "z"}.issubset(inspect.signature(ic_func).parameters):
+        raise ValueError("Initial condition function must accept x, y, z as arguments.")
+    if conservative_ic and fv_ic:
+        return NotImplemented, NotImplemented, ic_func
+    if fv_ic:
+        raise ValueError("Can't have finite volume averages without conservative IC.")
+    if conservative_ic:
+        w0f, u0 = NotImplemented, ic_func
+    else:
+        w0f = ic_func
+        u0 = lambda x, y, z: compute_conservatives(hs, ic_func(x, y, z), gamma=gamma)  # noqa: E731
+    return w0f, u0, lambda x, y, z: fv_average(u0, x, y, z, h=h, p=p)
+
+
+def initial_state(w0, nx: int, ny: int, nz: int = 1, px: int = 0, py: int = 0, pz: int = 0, x=(0, 1), y=(0, 1),
+                  z=(0, 1), gamma: float = 5 / 3, conservative_ic: bool = False, fv_ic: bool = False) -> np.ndarray:
+    """The conserved initial state (5, nx, ny, nz) float64 an EulerSolver with
+    these arguments starts from, without building the solver."""
+    n = (nx, ny, nz)
+    h = ((x[1] - x[0]) / nx, (y[1] - y[0]) / ny, (z[1] - z[0]) / nz)
+    X, Y, Z = fv_uniform_meshgen(n, x, y, z)
+    _, _, u0_fv = _ic_functions(w0, HydroState(), None, conservative_ic, fv_ic, gamma, h, (px, py, pz))
+    return np.ascontiguousarray(u0_fv(X, Y, Z), dtype=np.float64)
+
+
 class EulerSolver(ODE):
     def __init__(
         self,
@@ -155,23 +184,8 @@ class EulerSolver(ODE):
         self.hydro_state = HydroState(passive_scalars=passives)
         hs = self.hydro_state
         self.nvars = hs.nvars
-        ic_func = w0.build_ic(hs, w0_passives)
-        if not {"x", "y", "z"}.issubset(inspect.signature(ic_func).parameters):
-            raise ValueError("Initial condition function must accept x, y, z as arguments.")
-        if conservative_ic and fv_ic:
-            self.w0 = NotImplemented
-            self.u0 = NotImplemented
-            self.u0_fv = ic_func
-        elif fv_ic:
-            raise ValueError("Can't have finite volume averages without conservative IC.")
-        else:
-            if conservative_ic:
-                self.w0 = NotImplemented
-                self.u0 = ic_func
-            else:
-                self.w0 = ic_func
-                self.u0 = lambda x, y, z: compute_conservatives(hs, ic_func(x, y, z), gamma=self.gamma)
-            self.u0_fv = lambda x, y, z: fv_average(self.u0, x, y, z, h=self.h, p=self.p)
+        self.w0, self.u0, self.u0_fv = _ic_functions(w0, hs, w0_passives, conservative_ic, fv_ic, self.gamma, self.h,
+                                                     self.p)
         u0 = np.ascontiguousarray(self.u0_fv(self.X, self.Y, self.Z), dtype=np.float64)
         self._ode_init(progress_bar)
         self.am = ArrayManager(backend="cuda")

@@ -296,6 +296,57 @@ int fvh_get_pred_stats(fvh_handle* h, fvh_pred_stats* out, void* stream);
  * array flags. */
 int fvh_pred_flags(fvh_handle* h, uint8_t* flags, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Batched ensemble (no counterpart in the reference, which advances one
+ * problem per EulerSolver, fvhoe/ode.py:94-174): independent 2D problems that
+ * share every setting of cfg except the grid advance together, one
+ * cooperative persistent launch per SSP-RK3 stage over a work list of
+ * (problem, tile) entries, a whole step captured in a CUDA graph. Each member
+ * takes its own CFL dt, clamped to the common target, and stops when it
+ * reaches it, exactly as EulerSolver.ssprk3(t_end) does (fvhoe/ode.py:11-22,
+ * 94-112); an FP64 member equals the same problem run alone, bit for bit.
+ * cfg: the shared settings (cfg.n and cfg.h[0..1] are ignored; x and y must
+ * be active, five variables, equal p in 1..8 on x and y, no convex weights).
+ * ------------------------------------------------------------------------ */
+typedef struct fvh_ensemble fvh_ensemble;
+
+int fvh_ensemble_create(const fvh_config* cfg, int nprob, const int* nx, const int* ny, const double* hx,
+                        const double* hy, fvh_ensemble** out);
+int fvh_ensemble_destroy(fvh_ensemble* e);
+const char* fvh_ensemble_last_error(const fvh_ensemble* e);
+/* Device memory held by the ensemble (states and scratch). */
+size_t fvh_ensemble_bytes(const fvh_ensemble* e);
+/* Device pointer of member q's state, float64 (5, nx, ny); NULL for a bad q.
+ * Fill it before fvh_ensemble_reset / fvh_ensemble_step. */
+double* fvh_ensemble_state(fvh_ensemble* e, int q);
+/* Copies member q's state from src / to dst (host or device pointers of
+ * 5 * nx * ny doubles); store synchronises the stream. */
+int fvh_ensemble_load(fvh_ensemble* e, int q, const double* src, void* stream);
+int fvh_ensemble_store(fvh_ensemble* e, int q, double* dst, void* stream);
+/* Every member to time t0 with target t_end (active while t < t_end);
+ * synchronises the stream. */
+int fvh_ensemble_reset(fvh_ensemble* e, double t0, double t_end, void* stream);
+/* nsteps SSP-RK3 steps of every active member, stream-ordered after the
+ * caller's prior work on stream; no host synchronisation. */
+int fvh_ensemble_step(fvh_ensemble* e, int nsteps, void* stream);
+/* Per-member times and step counts (host arrays of nprob, each may be NULL),
+ * the number of active members and the non-finite values written since the
+ * reset; synchronises. FVH_ERR_TIMEOUT when a grid-barrier wait ran out. */
+int fvh_ensemble_status(fvh_ensemble* e, double* t, int* steps, int* active, unsigned int* nonfinite,
+                        void* stream);
+/* Tile shape variant (0..2 of fvh_ensemble_variant_info), resident blocks per
+ * SM of the persistent kernel (0 = as many as fit) and whether steps replay a
+ * captured CUDA graph. */
+int fvh_ensemble_configure(fvh_ensemble* e, int variant, int blocks_per_sm, int use_graph);
+int fvh_ensemble_variant_info(fvh_ensemble* e, int variant, int* tx, int* ty, int* max_blocks_per_sm,
+                              size_t* smem_bytes);
+/* Times `steps` steps of every variant and block count on the ensemble's own
+ * data (restoring states and times after each trial) and keeps the fastest. */
+int fvh_ensemble_autotune(fvh_ensemble* e, int steps, int* variant_out, int* blocks_out, double* ms_per_step,
+                          void* stream);
+/* Whether steps replay a CUDA graph, and why not when capture failed. */
+int fvh_ensemble_graph_info(const fvh_ensemble* e, int* in_use, const char** error);
+
 #ifdef __cplusplus
 }
 #endif

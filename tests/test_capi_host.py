@@ -67,6 +67,27 @@ def test_predictor_entry_points_refuse_null_arguments():
     assert _capi.lib.fvh_pred_flags(None, None, None) == _capi.ERR_ARG
 
 
+def test_ensemble_entry_points_refuse_bad_arguments():
+    import ctypes
+
+    from fvhoe_b200 import _capi
+
+    cfg = _capi.default_config()
+    out = ctypes.c_void_p()
+    n = (ctypes.c_int * 1)(32)
+    h = (ctypes.c_double * 1)(1 / 32)
+    assert _capi.lib.fvh_ensemble_create(None, 1, n, n, h, h, ctypes.byref(out)) == _capi.ERR_ARG
+    assert _capi.lib.fvh_ensemble_create(ctypes.byref(cfg), 0, n, n, h, h, ctypes.byref(out)) == _capi.ERR_ARG
+    # a 1D template cannot make 2D members
+    cfg.p[0], cfg.p[1], cfg.p[2] = 3, 0, 0
+    st = _capi.lib.fvh_ensemble_create(ctypes.byref(cfg), 1, n, (ctypes.c_int * 1)(1), h, h, ctypes.byref(out))
+    assert st == _capi.ERR_CONFIG and not out.value
+    assert _capi.lib.fvh_ensemble_destroy(None) == _capi.OK
+    assert _capi.lib.fvh_ensemble_state(None, 0) is None
+    assert _capi.lib.fvh_ensemble_step(None, 1, None) == _capi.ERR_ARG
+    assert _capi.lib.fvh_ensemble_status(None, None, None, None, None, None) == _capi.ERR_ARG
+
+
 def test_default_config_matches_reference_defaults():
     from fvhoe_b200 import _capi
 
