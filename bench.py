@@ -56,6 +56,10 @@ def parse():
     ap.add_argument("--pred-snapshots", type=int, default=16, help="stages sampled per training run")
     ap.add_argument("--pred-epochs", type=int, default=2)
     ap.add_argument("--pred-accuracy-time", type=float, default=0.002)
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
+    ap.add_argument("--ens-members", type=int, default=256)
+    ap.add_argument("--ens-steps", type=int, default=10, help="timed ensemble steps")
+    ap.add_argument("--ens-singles", type=int, default=16, help="members also timed one at a time")
     return ap.parse_args()
 
 
@@ -394,6 +398,95 @@ def predictor_leg(args, stream, sp):
     }
 
 
+def ensemble_members(count, seed=2024):
+    """The batched-ensemble workload: square grids of side drawn uniformly from
+    {128, 192, ..., 1024}, each a four-quadrant Riemann problem with its own
+    seeded split point and states."""
+    import numpy as np
+
+    from fvhoe_b200 import FourQuadrant2D
+
+    rng = np.random.default_rng(seed)
+    sides = rng.choice(np.arange(128, 1025, 64), size=count)
+    return [dict(w0=FourQuadrant2D(seed=1000 + q), nx=int(s), ny=int(s)) for q, s in enumerate(sides)]
+
+
+ENSEMBLE_KW = dict(gamma=1.4, riemann_solver="hllc", CFL=0.8, a_posteriori_slope_limiting=True, NAD=1e-5)
+
+
+def ensemble_leg(args, stream):
+    """256 independent four-quadrant problems (p=3, HLLC, SSP-RK3, CFL 0.8,
+    outflow, a-posteriori NAD 1e-5 + PAD + SED, FP32 with FP64 stage
+    accumulation), target t_end = 0.2 each: autotuned tile shape and blocks per
+    SM, CUDA-event time of ens_steps graph-replayed steps of the whole
+    ensemble; then a sample of the members timed one at a time through the
+    single-problem fused path, for the batching gain."""
+    import torch
+
+    from fvhoe_b200 import BoundaryCondition, Ensemble, EulerSolver
+
+    members = ensemble_members(args.ens_members)
+    kw = dict(ENSEMBLE_KW, bc=BoundaryCondition(x="outflow", y="outflow"))
+    t0 = time.perf_counter()
+    ens = Ensemble(members, px=3, precision="fp32", **kw)
+    t_setup = time.perf_counter() - t0
+    ens.reset(0.2)
+    tune = ens.autotune(steps=2)
+    ens.reset(0.2)
+    ens.step(args.warmup)
+    torch.cuda.synchronize()
+    before = ens.status()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    ens.step(args.ens_steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    after = ens.status()
+    updates = after["cell_updates"] - before["cell_updates"]
+    value = updates / (ms / 1e3) / 1e6
+    graph = ens.graph_info()
+    cells = int(sum(m["nx"] * m["ny"] for m in members))
+    nbytes = ens.nbytes()
+    del ens
+    torch.cuda.empty_cache()
+    # the same members one at a time (sampled): one fvh_step per member per step
+    import numpy as np
+
+    rng = np.random.default_rng(7)
+    pick = sorted(rng.choice(len(members), size=min(args.ens_singles, len(members)), replace=False).tolist())
+    single_updates = 0
+    single_ms = 0.0
+    for q in pick:
+        m = members[q]
+        s = EulerSolver(w0=m["w0"], nx=m["nx"], ny=m["ny"], px=3, py=3, precision="fp32", progress_bar=False,
+                        log_troubles=False, **kw)
+        s.ssprk3(n=args.warmup)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        s.ssprk3(n=args.ens_steps)
+        b.record(stream)
+        torch.cuda.synchronize()
+        single_ms += a.elapsed_time(b)
+        single_updates += 3 * args.ens_steps * m["nx"] * m["ny"]
+        del s
+    single_value = single_updates / (single_ms / 1e3) / 1e6
+    return {
+        "config": f"{len(members)} four-quadrant Riemann problems, square sides uniform in {{128..1024 step 64}} "
+                  f"({cells} cells), p=3, HLLC, SSP-RK3, CFL 0.8, outflow, NAD 1e-5 + PAD + SED, FP32 with FP64 "
+                  "stage accumulation, t_end = 0.2 each",
+        "value": value, "unit": UNIT, "steps": args.ens_steps, "ms_per_step": ms / args.ens_steps,
+        "cell_updates": int(updates), "active_after": after["active"], "nonfinite": after["nonfinite"],
+        "autotune": tune, "graph": graph, "device_bytes": nbytes, "setup_seconds": t_setup,
+        "one_at_a_time": {"members": len(pick), "value": single_value,
+                          "path": "EulerSolver.ssprk3, one fused-path step per member and step (dt read back)"},
+        "batching_gain": value / single_value,
+    }
+
+
 def run_ours(args):
     import ctypes
 
@@ -535,6 +628,12 @@ def run_ours(args):
                 line["learned_predictor"] = predictor_leg(args, stream, sp)
             except Exception as exc:  # the headline line is printed whatever this leg does
                 line["learned_predictor"] = {"error": f"{type(exc).__name__}: {exc}"}
+        if world == 1 and not args.no_ensemble:
+            torch.cuda.empty_cache()
+            try:
+                line["batched_ensemble"] = ensemble_leg(args, stream)
+            except Exception as exc:
+                line["batched_ensemble"] = {"error": f"{type(exc).__name__}: {exc}"}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -13,6 +13,7 @@ same problem run alone, bit for bit.
 """
 
 import ctypes
+import os
 import sys
 from typing import Dict, Sequence
 
@@ -66,11 +67,18 @@ class Ensemble:
             raise _capi.FvhError(st, (_capi.lib.fvh_ensemble_last_error(None) or b"").decode())
         self._e = handle
         self.cells = np.array([int(m["nx"]) * int(m["ny"]) for m in self.members], dtype=np.int64)
-        for q, m in enumerate(self.members):
-            u0 = initial_state(m["w0"], int(m["nx"]), int(m["ny"]), 1, px, px, 0, m["x"], m["y"], (0, 1),
-                               gamma=self.gamma, conservative_ic=m.get("conservative_ic", False),
-                               fv_ic=m.get("fv_ic", False))
-            self._check(_capi.lib.fvh_ensemble_load(self._e, q, u0.ctypes.data_as(ctypes.c_void_p), None))
+
+        def build(m):
+            return initial_state(m["w0"], int(m["nx"]), int(m["ny"]), 1, px, px, 0, m["x"], m["y"], (0, 1),
+                                 gamma=self.gamma, conservative_ic=m.get("conservative_ic", False),
+                                 fv_ic=m.get("fv_ic", False))
+
+        # initial states on the host cores (NumPy releases the GIL in its array loops)
+        from concurrent.futures import ThreadPoolExecutor
+
+        with ThreadPoolExecutor(max_workers=max(1, min(16, os.cpu_count() or 1))) as pool:
+            for q, u0 in enumerate(pool.map(build, self.members)):
+                self._check(_capi.lib.fvh_ensemble_load(self._e, q, u0.ctypes.data_as(ctypes.c_void_p), None))
         self._check(_capi.lib.fvh_ensemble_configure(self._e, 0 if precision == "fp32" else 1, 0, int(use_graph)))
         self.t_end = None
 
