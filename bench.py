@@ -109,13 +109,22 @@ def dist_setup(args):
 
 
 def max_over_ranks(x, dist):
+    """The maximum of x over the ranks (on the GPU with NCCL, on the host with gloo)."""
     if dist is None:
         return x
     import torch
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_throughput(units_per_rank, ms_local, dist, world):
+    """Whole-job Mcell-updates/s of `world` replicas that each did units_per_rank
+    cell-updates: all units over the slowest rank's time. Returns (value, max ms)."""
+    ms = max_over_ranks(ms_local, dist)
+    return world * units_per_rank / (ms / 1e3) / 1e6, ms
 
 
 # ---------------------------------------------------------------------------
@@ -537,8 +546,7 @@ def run_ours(args):
     if dist is not None:
         dist.barrier()
     clocks = sampler.stop()
-    ms = max_over_ranks(ms, dist)
-    value = world * 3 * cells * args.steps / (ms / 1e3) / 1e6
+    value, ms = replica_throughput(3 * cells * args.steps, ms, dist, world)
 
     plain_line = None
     if plain is not None:
@@ -548,8 +556,7 @@ def run_ours(args):
         if dist is not None:
             dist.barrier()
         msp, _ = _time_steps(lib, _capi, hp, up, sp, stream, args.steps)
-        msp = max_over_ranks(msp, dist)
-        pv = world * 3 * cells * args.steps / (msp / 1e3) / 1e6
+        pv, msp = replica_throughput(3 * cells * args.steps, msp, dist, world)
         plain_line = {"value": pv, "ms_per_step": msp / args.steps, "speedup_of_chosen": value / pv}
         del plain
 
