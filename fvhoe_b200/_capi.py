@@ -20,7 +20,7 @@ ERR_TIMEOUT = -3
 ERR_NONFINITE = -4
 ERR_ARG = -5
 
-BC = {"periodic": 0, "outflow": 1, "reflective": 2, "free": 3}
+BC = {"periodic": 0, "outflow": 1, "reflective": 2, "free": 3, "dirichlet": 4}
 RIEMANN = {"hllc": 0, "llf": 1, "advection_upwind": 2}
 LIMITER = {"minmod": 0, "moncen": 1, None: 2}
 PRECISION = {"fp64": 0, "fp32": 1}
@@ -60,6 +60,8 @@ EXPORTS = (
     "fvh_set_predictor",
     "fvh_get_pred_stats",
     "fvh_pred_flags",
+    "fvh_boundary_layout",
+    "fvh_set_boundary_values",
     "fvh_ensemble_create",
     "fvh_ensemble_destroy",
     "fvh_ensemble_last_error",
@@ -197,6 +199,10 @@ def _load():
     lib.fvh_pred_flags.argtypes = [vp, vp, vp]
     ip = ctypes.POINTER(ctypes.c_int)
     up = ctypes.POINTER(ctypes.c_uint)
+    lib.fvh_boundary_layout.argtypes = [vp, ctypes.c_int, ctypes.c_int, ip, ip, ctypes.POINTER(ctypes.c_size_t)]
+    lib.fvh_boundary_layout.restype = ctypes.c_int
+    lib.fvh_set_boundary_values.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp]
+    lib.fvh_set_boundary_values.restype = ctypes.c_int
     lib.fvh_ensemble_create.argtypes = [ctypes.POINTER(FvhConfig), ctypes.c_int, ip, ip, dp, dp, ctypes.POINTER(vp)]
     lib.fvh_ensemble_destroy.argtypes = [vp]
     lib.fvh_ensemble_last_error.argtypes = [vp]

@@ -1,17 +1,24 @@
 """Boundary-condition specification (host side).
 
 Same constructor as fvhoe/boundary_conditions.py:154-229 (`BoundaryCondition`
-with x, y, z kinds given as one value or a (low, high) pair). The ghost cells
-themselves are never materialised: the CUDA kernels read the interior through
-per-axis index maps (periodic wrap, mirror, mirror with the normal momentum
-negated, or edge repeat), which is what the reference's slab copies produce.
+with x, y, z kinds given as one value or a (low, high) pair, and x_value,
+y_value, z_value for Dirichlet sides). The ghost cells themselves are never
+materialised: the CUDA kernels read the interior through per-axis index maps
+(periodic wrap, mirror, mirror with the normal momentum negated, or edge
+repeat), which is what the reference's slab copies produce, and read the
+ghost values of "dirichlet" and "ic" sides from arrays the solver evaluates
+at the reference's slab coordinates (fvhoe/boundary_conditions.py:18-55).
 """
 
 from dataclasses import dataclass, field
 from typing import Any, Tuple, Union
 
-SUPPORTED = ("periodic", "outflow", "reflective", "free")
-NOT_SUPPORTED = ("dirichlet", "ic", "special-case-double-mach-reflection-y=0")
+import numpy as np
+
+SUPPORTED = ("periodic", "outflow", "reflective", "free", "dirichlet", "ic")
+# the reference's own branch for this kind calls _set_free_bc without its first
+# argument (fvhoe/boundary_conditions.py:382), so it cannot run there either
+NOT_SUPPORTED = ("special-case-double-mach-reflection-y=0",)
 
 
 @dataclass
@@ -54,6 +61,10 @@ class BoundaryCondition:
                         raise ValueError(f"Unknown bc type '{kind}'")
                 if pair[1] == "periodic" and pair[0] != "periodic":
                     raise ValueError(f"a periodic high boundary on {dim} needs a periodic low boundary")
+                values = getattr(self, f"{dim}_value")
+                for kind, value in zip(pair, values):
+                    if kind == "dirichlet" and not (callable(value) or isinstance(value, np.ndarray)):
+                        raise ValueError(f"Invalid boundary of type '{value}'.")
             out.append(tuple(pair))
         return tuple(out)
 

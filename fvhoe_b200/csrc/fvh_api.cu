@@ -140,7 +140,7 @@ int configure(fvh_handle* h, const fvh_config* cfg, std::string& msg) {
     if (!h->active[a]) continue;
     for (int side = 0; side < 2; ++side) {
       const int k = cfg->bc[a][side];
-      if (k < FVH_BC_PERIODIC || k > FVH_BC_FREE) {
+      if (k < FVH_BC_PERIODIC || k > FVH_BC_DIRICHLET) {
         msg = "unsupported boundary kind";
         return FVH_ERR_CONFIG;
       }
@@ -151,7 +151,9 @@ int configure(fvh_handle* h, const fvh_config* cfg, std::string& msg) {
     }
     const int ghosts = h->gW + 2 * h->r[a];
     for (int side = 0; side < 2; ++side) {
-      if (cfg->bc[a][side] != FVH_BC_FREE && ghosts > cfg->n[a]) {
+      // mirrored and periodic ghosts copy interior cells; free and Dirichlet ones do not
+      const int k = cfg->bc[a][side];
+      if (k != FVH_BC_FREE && k != FVH_BC_DIRICHLET && ghosts > cfg->n[a]) {
         msg = "axis " + std::string(1, "xyz"[a]) + " has " + std::to_string(cfg->n[a]) +
               " cells, fewer than the " + std::to_string(ghosts) + " ghost cells this degree needs";
         return FVH_ERR_CONFIG;
@@ -272,7 +274,8 @@ void release(fvh_handle* h) {
   h->prof = nullptr;
   void* ptrs[] = {h->bufA, h->bufB, h->W,        h->Ws,       h->Us,       h->F[0],     h->F[1],
                   h->F[2], h->trouble, h->logs[0], h->logs[1], h->logs[2], h->acc,      h->S[0],
-                  h->S[1], h->theta[0], h->theta[1], h->theta[2], h->conv, h->sc, h->pred};
+                  h->S[1], h->theta[0], h->theta[1], h->theta[2], h->conv, h->sc, h->pred, h->slabs_dev,
+                  h->slab[0][0], h->slab[0][1], h->slab[1][0], h->slab[1][1], h->slab[2][0], h->slab[2][1]};
   for (void* p : ptrs)
     if (p) cudaFree(p);
 }
@@ -320,6 +323,34 @@ int allocate(fvh_handle* h) {
   if ((st = alloc(h, (void**)&h->S[1], state))) return st;
   if ((st = alloc(h, (void**)&h->sc, sizeof(fvh::Scalars)))) return st;
   cudaMemset(h->sc, 0, sizeof(fvh::Scalars));
+  // Dirichlet sides: ghost-value arrays (zero until the caller uploads) and their descriptor
+  bool dirichlet = false;
+  fvh::Slabs& m = h->slab_meta;
+  for (int a = 0; a < 3; ++a) {
+    m.n[a] = h->n[a];
+    m.depth[a] = h->active[a] ? h->gW + 2 * h->r[a] : 0;
+    m.pad[a] = m.depth[a];
+    for (int side = 0; side < 2; ++side) m.bc[a][side] = h->grid.bc[a][side];
+  }
+  for (int a = 0; a < 3; ++a) {
+    if (!h->active[a]) continue;
+    for (int side = 0; side < 2; ++side) {
+      if (h->cfg.bc[a][side] != FVH_BC_DIRICHLET) continue;
+      size_t count = nv * (size_t)m.depth[a];
+      for (int b = 0; b < 3; ++b)
+        if (b != a) count *= (size_t)(h->n[b] + 2 * m.pad[b]);
+      if ((st = alloc(h, (void**)&h->slab[a][side], count * sizeof(double)))) return st;
+      cudaMemset(h->slab[a][side], 0, count * sizeof(double));
+      h->slab_count[a][side] = count;
+      m.p[a][side] = h->slab[a][side];
+      dirichlet = true;
+    }
+  }
+  if (dirichlet) {
+    if ((st = alloc(h, (void**)&h->slabs_dev, sizeof(fvh::Slabs)))) return st;
+    cudaMemcpy(h->slabs_dev, &m, sizeof(fvh::Slabs), cudaMemcpyHostToDevice);
+    h->grid.slabs = h->slabs_dev;
+  }
   const cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     h->err = std::string("initialising scratch: ") + cudaGetErrorString(e);
@@ -563,6 +594,30 @@ int fvh_get_stats(fvh_handle* h, fvh_stats* out, void* stream) {
   out->dt_step = host.dt_step;
   out->troubled = host.troubled;
   out->nonfinite = host.nonfinite;
+  return FVH_OK;
+}
+
+int fvh_boundary_layout(fvh_handle* h, int axis, int side, int* depth, int* ext, size_t* count) {
+  if (!h) return FVH_ERR_ARG;
+  if (axis < 0 || axis > 2 || side < 0 || side > 1) return fail(h, FVH_ERR_ARG, "axis must be 0..2, side 0..1");
+  if (!h->slab[axis][side]) return fail(h, FVH_ERR_CONFIG, "that side is not a Dirichlet boundary");
+  const fvh::Slabs& m = h->slab_meta;
+  if (depth) *depth = m.depth[axis];
+  if (ext)
+    for (int b = 0; b < 3; ++b) ext[b] = b == axis ? m.depth[b] : h->n[b] + 2 * m.pad[b];
+  if (count) *count = h->slab_count[axis][side];
+  return FVH_OK;
+}
+
+int fvh_set_boundary_values(fvh_handle* h, int axis, int side, const double* values, void* stream) {
+  if (!h) return FVH_ERR_ARG;
+  if (axis < 0 || axis > 2 || side < 0 || side > 1 || !values)
+    return fail(h, FVH_ERR_ARG, "axis must be 0..2, side 0..1, values non-null");
+  if (!h->slab[axis][side]) return fail(h, FVH_ERR_CONFIG, "that side is not a Dirichlet boundary");
+  if (int st0 = use_device(h)) return st0;
+  const cudaError_t e = cudaMemcpyAsync(h->slab[axis][side], values, h->slab_count[axis][side] * sizeof(double),
+                                        cudaMemcpyDefault, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(h, FVH_ERR_CUDA, cudaGetErrorString(e));
   return FVH_OK;
 }
 

@@ -153,6 +153,12 @@ int fvh_ensemble_create(const fvh_config* cfg, int nprob, const int* nx, const i
       delete e;
       return fail(nullptr, st, "problem " + std::to_string(q) + ": " + msg);
     }
+    for (int a = 0; a < 2; ++a)
+      for (int side = 0; side < 2; ++side)
+        if (c.bc[a][side] == FVH_BC_DIRICHLET) {
+          delete e;
+          return fail(nullptr, FVH_ERR_CONFIG, "ensemble members cannot have Dirichlet boundaries");
+        }
     if (!tmp.active[0] || !tmp.active[1]) {
       delete e;
       return fail(nullptr, FVH_ERR_CONFIG, "ensemble members must have two active axes (x and y)");

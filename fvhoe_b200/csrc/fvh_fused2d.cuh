@@ -31,6 +31,7 @@ struct Geo {
   int bcx[2], bcy[2];  // Bc kinds at the low/high ends of X and Y
   int dx, dy;          // physical axis ids of X and Y
   int gmax;            // deepest ghost index any state load may reach
+  const Slabs* slabs;  // Dirichlet ghost values (physical axes), or nullptr
 };
 
 // 2D view of a variable-major array over [-g, nx+g) x [-g, ny'+g).
@@ -59,6 +60,15 @@ template <typename Tc>
 __device__ __forceinline__ void load_state2(const double* __restrict__ u, const Geo& g, int x, int y, Tc* out) {
   x = min(max(x, -g.gmax), g.nx + g.gmax - 1);
   y = min(max(y, -g.gmax), g.ny + g.gmax - 1);
+  if (g.slabs) {
+    int i[3] = {0, 0, 0};
+    i[g.dx] = x;
+    i[g.dy] = y;
+    const State5<Tc> s = load_state5_dirichlet<Tc>(u, g.slabs, i[0], i[1], i[2]);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) out[v] = s.v[v];
+    return;
+  }
   bool fx = false, fy = false;
   const int jx = ghost_source(x, g.nx, g.bcx[0], g.bcx[1], fx);
   const int jy = ghost_source(y, g.ny, g.bcy[0], g.bcy[1], fy);

@@ -40,6 +40,10 @@ struct fvh_handle {
   double* acc = nullptr;          // running k-sum of ssprk3 / rk4
   double* S[2] = {nullptr, nullptr};              // stage inputs
   fvh::Scalars* sc = nullptr;
+  double* slab[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};  // Dirichlet ghost values
+  size_t slab_count[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+  fvh::Slabs slab_meta{};                 // host copy of the descriptor
+  fvh::Slabs* slabs_dev = nullptr;        // device copy (grid.slabs points here)
   size_t scratch_bytes = 0;
 
   // learned troubled-cell predictor (optional)

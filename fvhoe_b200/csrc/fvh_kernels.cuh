@@ -25,16 +25,31 @@
 
 namespace fvh {
 
-enum Bc : int { BC_PERIODIC = 0, BC_OUTFLOW = 1, BC_REFLECTIVE = 2, BC_FREE = 3 };
+enum Bc : int { BC_PERIODIC = 0, BC_OUTFLOW = 1, BC_REFLECTIVE = 2, BC_FREE = 3, BC_DIRICHLET = 4 };
 
 struct Region {
   int lo[3];
   int n[3];
 };
 
+// Ghost values of Dirichlet sides (boundary kinds "dirichlet" and "ic",
+// fvhoe/boundary_conditions.py:18-55), given by the host: for axis a and side
+// s an array (nv, E0, E1, E2) with E_a = depth[a] ghost layers along a and
+// E_b = n_b + 2 pad[b] along the other axes (their ghost layers included).
+// Element (v, i) of a ghost cell i: along a, i_a + depth[a] on the low side and
+// i_a - n_a on the high side; along b, i_b + pad[b].
+struct Slabs {
+  int n[3];
+  int bc[3][2];
+  const double* p[3][2];  // nullptr unless that side is Dirichlet
+  int depth[3];
+  int pad[3];
+};
+
 struct Grid {
   int n[3];      // interior cells per axis
   int bc[3][2];  // Bc kinds at the low/high end of each axis
+  const Slabs* slabs;  // device copy when any side is Dirichlet, else nullptr
 };
 
 template <typename T, int K>
@@ -146,11 +161,83 @@ __device__ __forceinline__ int state_stride(const Grid& g, int axis) {
   return axis == 0 ? g.n[1] * g.n[2] : (axis == 1 ? g.n[2] : 1);
 }
 
+// Conserved state at a (possibly ghost) cell i when some side is Dirichlet.
+// The reference fills the ghost slabs axis after axis, x then y then z, each
+// slab spanning the others' ghost layers (fvhoe/boundary_conditions.py:306-402),
+// so the last axis decides a corner: resolve z, then y, then x. A Dirichlet
+// side returns its slab value at the coordinates mapped so far; a mirrored,
+// periodic or free side maps its coordinate into the interior (the reflective
+// sign flips apply to whatever value ends up copied).
+template <typename Tc>
+__device__ __forceinline__ void dirichlet_core(const double* __restrict__ u, const Slabs* __restrict__ sl, int nv,
+                                               int i0, int i1, int i2, Tc* out) {
+  int i[3] = {i0, i1, i2};
+  bool flip[3] = {false, false, false};
+  for (int a = 2; a >= 0; --a) {
+    const int ia = i[a];
+    const int na = sl->n[a];
+    if (ia >= 0 && ia < na) continue;
+    const int side = ia < 0 ? 0 : 1;
+    if (sl->bc[a][side] == BC_DIRICHLET) {
+      int e[3], k[3];
+      for (int b = 0; b < 3; ++b) {
+        e[b] = b == a ? sl->depth[b] : sl->n[b] + 2 * sl->pad[b];
+        k[b] = b == a ? (side == 0 ? ia + sl->depth[b] : ia - na) : i[b] + sl->pad[b];
+      }
+      const double* p = sl->p[a][side];
+      const int plane = e[0] * e[1] * e[2];
+      const int o = (k[0] * e[1] + k[1]) * e[2] + k[2];
+      for (int v = 0; v < nv; ++v) {
+        double x = p[v * plane + o];
+        if ((v == 1 && flip[0]) || (v == 2 && flip[1]) || (v == 3 && flip[2])) x = -x;
+        out[v] = (Tc)x;
+      }
+      return;
+    }
+    bool f = false;
+    i[a] = ghost_source(ia, na, sl->bc[a][0], sl->bc[a][1], f);
+    flip[a] = f;
+  }
+  const int plane = sl->n[0] * sl->n[1] * sl->n[2];
+  const int o = (i[0] * sl->n[1] + i[1]) * sl->n[2] + i[2];
+  for (int v = 0; v < nv; ++v) {
+    double x = u[v * plane + o];
+    if ((v == 1 && flip[0]) || (v == 2 && flip[1]) || (v == 3 && flip[2])) x = -x;
+    out[v] = (Tc)x;
+  }
+}
+
+// Out-of-line wrappers, so that kernels without Dirichlet sides pay only a
+// uniform branch: any number of variables through a pointer, and the five
+// variables of the fused 2D path returned by value (in registers).
+template <typename Tc>
+__device__ __noinline__ void load_state_dirichlet(const double* __restrict__ u, const Slabs* __restrict__ sl, int nv,
+                                                  int i0, int i1, int i2, Tc* out) {
+  dirichlet_core<Tc>(u, sl, nv, i0, i1, i2, out);
+}
+
+template <typename Tc>
+struct State5 {
+  Tc v[5];
+};
+
+template <typename Tc>
+__device__ __noinline__ State5<Tc> load_state5_dirichlet(const double* __restrict__ u, const Slabs* __restrict__ sl,
+                                                         int i0, int i1, int i2) {
+  State5<Tc> s;
+  dirichlet_core<Tc>(u, sl, 5, i0, i1, i2, s.v);
+  return s;
+}
+
 // Reads nv conserved variables at a (possibly ghost) cell. Reflective ghosts
 // negate the momentum normal to the wall they mirror across.
 template <typename Tc>
 __device__ __forceinline__ void load_state(const double* __restrict__ u, const Grid& g, int nv, int i0, int i1,
                                            int i2, Tc* out) {
+  if (g.slabs) {
+    load_state_dirichlet<Tc>(u, g.slabs, nv, i0, i1, i2, out);
+    return;
+  }
   bool f0 = false, f1 = false, f2 = false;
   const int j0 = ghost_source(i0, g.n[0], g.bc[0][0], g.bc[0][1], f0);
   const int j1 = ghost_source(i1, g.n[1], g.bc[1][0], g.bc[1][1], f1);
@@ -272,6 +359,17 @@ __global__ void __launch_bounds__(256)
     Tc acc[NVA];
     for (int v = 0; v < nv; ++v) acc[v] = Tc(0);
     if constexpr (FROM_STATE) {
+      if (grid.slabs) {
+        // Dirichlet sides: every tap through the general ghost resolution
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          int t[3] = {i[0], i[1], i[2]};
+          t[axis] += rule.off + k;
+          Tc uc[NVA];
+          load_state_dirichlet<Tc>(state, grid.slabs, nv, t[0], t[1], t[2], uc);
+          for (int v = 0; v < nv; ++v) acc[v] = acc[v] + rule.w[k] * uc[v];
+        }
+      } else {
       // ghost maps of the two fixed coordinates, once per point
       bool fl[3] = {false, false, false};
       int base = 0;
@@ -298,6 +396,7 @@ __global__ void __launch_bounds__(256)
           if (flip) x = -x;
           acc[v] = acc[v] + rule.w[k] * (Tc)x;
         }
+      }
       }
     } else {
       const int sa = in.stride(axis);

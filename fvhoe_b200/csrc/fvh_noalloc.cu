@@ -83,6 +83,10 @@ int fvh_primitives_noalloc(const fvh_config* cfg, const double* u, double* w, in
   const int st = fvh::configure_handle(&h, cfg, msg);
   if (st) return set_error(st, msg.c_str());
   if (h.cfg.device >= kMaxDevices) return set_error(FVH_ERR_CONFIG, "device ordinal too large");
+  for (int a = 0; a < 3; ++a)
+    for (int side = 0; side < 2; ++side)
+      if (h.active[a] && cfg->bc[a][side] == FVH_BC_DIRICHLET)
+        return set_error(FVH_ERR_CONFIG, "Dirichlet boundaries need a handle (fvh_primitives) for their ghost values");
   // per-buffer requirement: the state ghost-filled by 2r on each active axis
   size_t need = (size_t)h.nv;
   for (int a = 0; a < 3; ++a) need *= (size_t)(h.n[a] + (h.active[a] ? 4 * h.r[a] : 0));

@@ -588,6 +588,7 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
   g.dx = ax[0];
   g.dy = ax[1];
   g.gmax = h->gW + 2 * h->r[ax[0]];
+  g.slabs = h->grid.slabs;
   const Rule<Tc, KC> crule = device_rule<Tc, KC>(centre_rule(P));
   const Rule<Tc, KC> trule = device_rule<Tc, KC>(transverse_rule(P));
   const Rule<Tc, KF> lrule = device_rule<Tc, KF>(left_face_rule(P));

@@ -1,12 +1,14 @@
 """Mesh and finite-volume averaging of initial conditions (host, set-up only).
 
-Same interfaces as fvhoe/fv.py:12-85 (`fv_uniform_meshgen` without slab
-coordinates) and :227-277 (`fv_average` with Gauss-Legendre quadrature).
-These run once per solver, on the host, before the state moves to the GPU.
+Same interfaces as fvhoe/fv.py:12-85 (`fv_uniform_meshgen`; the ghost-slab
+coordinates are `slab_meshgen`) and :227-277 (`fv_average` with
+Gauss-Legendre quadrature). These run on the host: the averaging once per
+solver, the slab coordinates once per solver with Dirichlet boundaries.
 """
 
 from functools import lru_cache
-from typing import Callable, Tuple
+from itertools import product
+from typing import Callable, Dict, Tuple
 
 import numpy as np
 
@@ -18,6 +20,40 @@ def fv_uniform_meshgen(n, x=(0, 1), y=(0, 1), z=(0, 1)):
         edges = np.linspace(lo, hi, count + 1)
         centres.append(0.5 * (edges[1:] + edges[:-1]))
     return np.meshgrid(*centres, indexing="ij")
+
+
+def slab_meshgen(n, x=(0, 1), y=(0, 1), z=(0, 1), thickness=(0, 0, 0)) -> Dict[str, tuple]:
+    """Cell centres of the ghost slabs {'xl': (X, Y, Z), 'xr': ..., 'zr': ...}
+    built as fvhoe/fv.py:53-84 builds them: each slab is `thickness` cells deep
+    along its axis and spans the other axes with their slabs included."""
+    h = ((x[1] - x[0]) / n[0], (y[1] - y[0]) / n[1], (z[1] - z[0]) / n[2])
+    gwx, gwy, gwz = thickness
+    out = {}
+    for dim, pos in product("xyz", "lr"):
+        sizes = (gwx if dim == "x" else n[0] + 2 * gwx, gwy if dim == "y" else n[1] + 2 * gwy,
+                 gwz if dim == "z" else n[2] + 2 * gwz)
+        ranges = []
+        for d, (lo, hi), hd, gd in zip("xyz", (x, y, z), h, thickness):
+            if d == dim:
+                ranges.append({"l": (lo - hd * gd, lo), "r": (hi, hi + hd * gd)}[pos])
+            else:
+                ranges.append((lo - hd * gd, hi + hd * gd))
+        out[dim + pos] = tuple(fv_uniform_meshgen(sizes, *ranges))
+    return out
+
+
+def trim_slab(coords, buffer, gw, axis: int, pos: str):
+    """The part of a slab (from slab_meshgen with thickness `buffer`) that a
+    ghost fill of width gw uses: the gw layers next to the domain along `axis`,
+    the interior plus gw layers along the others (fvhoe/boundary_conditions.py:231-289)."""
+    sl = []
+    for a in range(3):
+        excess = buffer[a] - gw[a]
+        if excess < 0:
+            raise ValueError(f"Cannot apply bc to region of thickness {gw[a]} with a buffer of thickness {buffer[a]}")
+        cut = {"l": (-gw[a], 0), "r": (0, gw[a])}[pos] if a == axis else (excess, -excess)
+        sl.append(slice(cut[0] or None, cut[1] or None))
+    return tuple(c[tuple(sl)] for c in coords)
 
 
 @lru_cache(maxsize=16)

@@ -229,6 +229,8 @@ class EulerSolver(ODE):
             cfg.h[a] = self.h[a]
             for side in range(2):
                 kind = self._bc_kinds[a][side]
+                if kind == "ic":
+                    kind = "dirichlet"
                 cfg.bc[a][side] = c.BC.get(kind, 0) if kind is not None else 0
         cfg.gamma = self.gamma
         cfg.cfl = self.CFL
@@ -276,6 +278,78 @@ class EulerSolver(ODE):
         self._handle = handle
         self._predictor = None
         self.pred_totals = None
+        self._init_dirichlet()
+
+    # -- Dirichlet and "ic" boundaries (fvhoe/boundary_conditions.py:18-55, 334-347) --------
+    def _init_dirichlet(self):
+        """Slab coordinates of every Dirichlet side, built like the reference
+        (slab_buffer_size cells on the active axes, fvhoe/solver.py:318-361),
+        trimmed to the ghost depth the kernels read, and the static values."""
+        self._dirichlet = []
+        active = (self.xdim, self.ydim, self.zdim)
+        sides = [(a, s) for a in range(3) if active[a] for s in range(2)
+                 if self._bc_kinds[a][s] in ("dirichlet", "ic")]
+        if not sides:
+            return
+        from .fv import slab_meshgen, trim_slab
+
+        c = self._capi
+        # ghost layers along every active axis (the slabs span the other axes' ghost layers too)
+        depth = [self.gW_depth(a) if active[a] else 0 for a in range(3)]
+        for a, s in sides:
+            d = ctypes.c_int()
+            c.check(c.lib.fvh_boundary_layout(self._handle, a, s, ctypes.byref(d), None, None), self._handle)
+            if d.value != depth[a]:
+                raise RuntimeError(f"ghost depth mismatch on axis {a}: library {d.value}, host {depth[a]}")
+        buffer = tuple(self.slab_buffer_size if on else 0 for on in active)
+        coords = slab_meshgen(self.n, self.x_domain, self.y_domain, self.z_domain, buffer)
+        for a, s in sides:
+            dim, pos = "xyz"[a], "lr"[s]
+            X, Y, Z = trim_slab(coords[dim + pos], buffer, tuple(depth), a, pos)
+            kind = self._bc_kinds[a][s]
+            value = getattr(self.bc, f"{dim}_value")[s]
+            if kind == "ic":
+                if self.u0 is NotImplemented:
+                    raise ValueError("'ic' boundaries need a pointwise conservative initial condition")
+                value = self.u0
+            self._dirichlet.append(dict(axis=a, side=s, kind=kind, value=value, coords=(X, Y, Z)))
+        self._dirichlet_dynamic = any(d["kind"] == "dirichlet" and callable(d["value"]) for d in self._dirichlet)
+        self._upload_boundaries(force=True)
+
+    def gW_depth(self, a: int) -> int:
+        """Ghost layers the kernels read along axis a: max(gw, 3 if limiting) + 2 ceil(p_a / 2)."""
+        p = [pi for pi, on in zip(self.p, (self.xdim, self.ydim, self.zdim)) if on]
+        r = -(-max(p) // 2)
+        gw = max(r + 1, 2 * r)
+        if self.a_posteriori_slope_limiting:
+            gw = max(gw, 3)
+        return gw + 2 * (-(-self.p[a] // 2))
+
+    def _upload_boundaries(self, force=False):
+        if not self._dirichlet or not (force or self._dirichlet_dynamic):
+            return
+        c = self._capi
+        for d in self._dirichlet:
+            X, Y, Z = d["coords"]
+            value = d["value"]
+            if d["kind"] == "ic":
+                if not force:
+                    continue
+                vals = value(x=X, y=Y, z=Z)
+            elif callable(value):
+                vals = value(x=X, y=Y, z=Z, t=self.t)
+            else:
+                vals = np.ones((self.nvars,) + X.shape) * np.asarray(value).reshape(-1, 1, 1, 1)
+            vals = np.ascontiguousarray(vals, dtype=np.float64)
+            count = ctypes.c_size_t()
+            c.check(c.lib.fvh_boundary_layout(self._handle, d["axis"], d["side"], None, None, ctypes.byref(count)),
+                    self._handle)
+            if vals.size != count.value:
+                raise ValueError(f"boundary values of shape {vals.shape} do not fill the {count.value} ghost values "
+                                 f"of side {'xyz'[d['axis']]}{'lr'[d['side']]}")
+            c.check(c.lib.fvh_set_boundary_values(self._handle, d["axis"], d["side"],
+                                                  vals.ctypes.data_as(ctypes.c_void_p), self._stream()),
+                    self._handle)
 
     # -- learned troubled-cell predictor (no counterpart in the reference) ------
     def set_predictor(self, predictor, threshold: float = 0.5):
@@ -365,6 +439,7 @@ class EulerSolver(ODE):
         u = self._as_device(u)
         dudt = torch.empty_like(u)
         dt = ctypes.c_double()
+        self._upload_boundaries()
         self._set_log_mode()
         self._capi.check(
             self._capi.lib.fvh_rhs(self._handle, ctypes.c_void_p(u.data_ptr()), ctypes.c_void_p(dudt.data_ptr()),
@@ -384,6 +459,7 @@ class EulerSolver(ODE):
             raise ValueError(f"unknown integrator {integrator}")
         u = self.am("u")
         dt = ctypes.c_double()
+        self._upload_boundaries()
         self._set_log_mode()
         self._capi.check(
             self._capi.lib.fvh_step(

@@ -47,6 +47,7 @@ extern "C" {
 #define FVH_BC_OUTFLOW 1 /* mirror */
 #define FVH_BC_REFLECTIVE 2 /* mirror, normal momentum negated */
 #define FVH_BC_FREE 3 /* repeat the edge cell */
+#define FVH_BC_DIRICHLET 4 /* ghost values given by the caller ("dirichlet" and "ic") */
 
 /* Riemann solvers (fvhoe/solver.py:185-193) */
 #define FVH_RIEMANN_HLLC 0
@@ -171,6 +172,19 @@ int fvh_primitives(fvh_handle* h, const double* u, double* w, int fv_average, vo
 int fvh_primitives_noalloc(const fvh_config* cfg, const double* u, double* w, int fv_average, void* stream);
 size_t fvh_primitives_noalloc_max_doubles(void);
 const char* fvh_primitives_noalloc_error(void);
+
+/* Ghost values of a Dirichlet side (FVH_BC_DIRICHLET: the reference's
+ * "dirichlet" and "ic" kinds, fvhoe/boundary_conditions.py:18-55, 334-347).
+ * The layout of side (axis, side): nvars x ext[0] x ext[1] x ext[2] doubles,
+ * ext[axis] = *depth ghost layers ordered outward-in on the low side
+ * (cell -depth first) and inward-out on the high side (cell n first), the other
+ * active axes spanning their interior plus `depth` ghost layers on each side
+ * (ext = n + 2 * depth), inactive axes 1. The reference evaluates its boundary
+ * functions at these cells' centres once per step (t = the step's start time);
+ * the caller does the same and uploads with fvh_set_boundary_values (host or
+ * device pointer) before the step. */
+int fvh_boundary_layout(fvh_handle* h, int axis, int side, int* depth, int* ext, size_t* count);
+int fvh_set_boundary_values(fvh_handle* h, int axis, int side, const double* values, void* stream);
 
 /* Copies the trouble flags of the last stage (uint8, nx*ny*nz) to the device
  * array flags. Replaces the troubled_cells array of revise_fluxes

@@ -169,7 +169,12 @@ class OracleConfig:
 
     Mirrors the constructor arguments of fvhoe/solver.py:42-84 that reach the
     hot path; `bc` holds (low, high) kinds per axis from
-    {"periodic", "outflow", "reflective", "free"}.
+    {"periodic", "outflow", "reflective", "free", "dirichlet", "ic"};
+    `bc_values` the value of each "dirichlet" side (an array of nvars
+    conserved values, or a function of x, y, z, t) and of each "ic" side (the
+    pointwise conserved initial condition, a function of x, y, z); `t` is the
+    time the boundary functions see (the step's start time,
+    fvhoe/solver.py:784).
     """
 
     n: Tuple[int, int, int]
@@ -199,6 +204,10 @@ class OracleConfig:
     SED_tolerance: float = 1e-10
     convex: bool = False
     csq_floor: float = 1e-10
+    domain: Tuple[Tuple[float, float], ...] = ((0.0, 1.0), (0.0, 1.0), (0.0, 1.0))
+    bc_values: Optional[Tuple] = None
+    slab_buffer_size: int = 30
+    t: float = 0.0
 
     @property
     def active(self) -> Tuple[bool, bool, bool]:
@@ -242,25 +251,88 @@ def _ghost_source(n: int, g: int, low: str, high: str):
     return src, flip
 
 
-def pad_with_ghosts(u: np.ndarray, g: Sequence[int], bc) -> np.ndarray:
+def _slab_meshgen(n, domain, thickness):
+    """Cell centres of the ghost slabs, {'xl': (X, Y, Z), ...} (fvhoe/fv.py:53-84)."""
+    def centres(count, lo, hi):
+        edges = np.linspace(lo, hi, count + 1)
+        return 0.5 * (edges[1:] + edges[:-1])
+
+    h = [(domain[a][1] - domain[a][0]) / n[a] for a in range(3)]
+    out = {}
+    for a, dim in enumerate("xyz"):
+        for pos in "lr":
+            axes = []
+            for b in range(3):
+                lo, hi = domain[b]
+                gb = thickness[b]
+                if b == a:
+                    rng = (lo - h[b] * gb, lo) if pos == "l" else (hi, hi + h[b] * gb)
+                    axes.append(centres(gb, *rng))
+                else:
+                    axes.append(centres(n[b] + 2 * gb, lo - h[b] * gb, hi + h[b] * gb))
+            out[dim + pos] = tuple(np.meshgrid(*axes, indexing="ij"))
+    return out
+
+
+def _dirichlet_slab(cfg, axis: int, side: int, g: Sequence[int]) -> np.ndarray:
+    """Ghost values of a "dirichlet" or "ic" side for a fill of g cells per
+    axis (fvhoe/boundary_conditions.py:18-55, 231-289, 334-347): the slab
+    coordinates are built slab_buffer_size deep and trimmed to g."""
+    buffer = tuple(cfg.slab_buffer_size if act else 0 for act in cfg.active)
+    pos = "lr"[side]
+    coords = _slab_meshgen(cfg.n, cfg.domain, buffer)["xyz"[axis] + pos]
+    sl = []
+    for a in range(3):
+        excess = buffer[a] - g[a]
+        cut = ((-g[a], 0) if pos == "l" else (0, g[a])) if a == axis else (excess, -excess)
+        sl.append(slice(cut[0] or None, cut[1] or None))
+    X, Y, Z = (c[tuple(sl)] for c in coords)
+    kind = cfg.bc[axis][side]
+    value = cfg.bc_values[axis][side]
+    if kind == "ic":
+        return value(x=X, y=Y, z=Z)
+    if callable(value):
+        return value(x=X, y=Y, z=Z, t=cfg.t)
+    return np.ones((cfg.nvars,) + X.shape) * np.asarray(value).reshape(-1, 1, 1, 1)
+
+
+def pad_with_ghosts(u: np.ndarray, g: Sequence[int], bc, cfg=None) -> np.ndarray:
     """Pad (nvars, nx, ny, nz) by g[a] ghost cells per spatial axis.
 
     periodic copies the opposite interior, outflow mirrors, reflective mirrors
     and negates the normal momentum, free repeats the edge cell
-    (fvhoe/boundary_conditions.py:60-151); axes are filled x, then y, then z,
-    so corner ghosts compose the per-axis maps (:324-400).
+    (fvhoe/boundary_conditions.py:60-151), "dirichlet" and "ic" sides take
+    the values of cfg (:18-55); axes are filled x, then y, then z, each slab
+    spanning the ghost layers of the axes filled before it, so corner ghosts
+    take the last axis' treatment of the earlier axes' values (:324-400).
     """
     out = u
     for axis in range(3):
         if g[axis] == 0:
             continue
-        src, flip = _ghost_source(out.shape[axis + 1], g[axis], *bc[axis])
+        kinds = list(bc[axis])
+        dirichlet = [k in ("dirichlet", "ic") for k in kinds]
+        mapped = [k if not d else "free" for k, d in zip(kinds, dirichlet)]
+        n_a = out.shape[axis + 1]
+        src, flip = _ghost_source(n_a, g[axis], *mapped)
         out = np.take(out, src, axis=axis + 1)
         if flip.any():
             sel = [slice(None)] * 4
             sel[0] = 1 + axis
             sel[axis + 1] = flip
             out[tuple(sel)] *= -1.0
+        for side in range(2):
+            if not dirichlet[side]:
+                continue
+            values = _dirichlet_slab(cfg, axis, side, g)
+            # the axes after this one are not padded yet: their interior part
+            sel = [slice(None)] * 4
+            for b in range(axis + 1, 3):
+                sel[b + 1] = slice(g[b], g[b] + cfg.n[b])
+            values = values[tuple(sel)]
+            dst = [slice(None)] * 4
+            dst[axis + 1] = slice(0, g[axis]) if side == 0 else slice(n_a + g[axis], n_a + 2 * g[axis])
+            out[tuple(dst)] = values
     return out
 
 
@@ -333,7 +405,7 @@ def fv_primitives(
     """
     factor = 2 if fv_average else 1
     g = [gw[a] + factor * stencil_radius(p[a]) for a in range(3)]
-    a_bc = pad_with_ghosts(u, g, cfg.bc)
+    a_bc = pad_with_ghosts(u, g, cfg.bc, cfg)
     for axis in range(3):
         a_bc = sweep(a_bc, stencil_weights(p[axis], "c"), axis + 1)
     w = conservatives_to_primitives(a_bc, cfg.gamma)
@@ -797,7 +869,11 @@ def hit_target(t: float, dt: float, target: Optional[float]) -> float:
 
 
 def step(u: np.ndarray, t: float, cfg: OracleConfig, integrator: str = "ssprk3", target=None):
-    """One time step; returns (dt, u_next, per-stage infos) (fvhoe/ode.py:245-298)."""
+    """One time step; returns (dt, u_next, per-stage infos) (fvhoe/ode.py:245-298).
+    Boundary functions see the step's start time in every stage (fvhoe/solver.py:784)."""
+    from dataclasses import replace
+
+    cfg = replace(cfg, t=t)
     infos = []
 
     def f(x):

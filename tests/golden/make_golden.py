@@ -29,6 +29,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 def _setup(reference):
     sys.path.insert(0, reference)
     sys.path.insert(0, os.path.join(HERE, "_mpl_stub"))
+    sys.path.insert(0, HERE)
 
 
 def _json_pad(pad):
@@ -169,6 +170,22 @@ def build_cases():
     for integ in ("euler", "ssprk2", "rk4"):
         add("steps", f"shock_x_p2_{integ}", shock("x"), (64, 1, 1), (2, 0, 0), steps=3, integrator=integ,
             gamma=1.4, bc=dict(x="outflow"), riemann_solver="hllc", **lim)
+    # Dirichlet and "ic" boundaries (values named in bc_values.py; "ic" sides use the
+    # initial condition named by ic_spec)
+    add("steps", "sod_ic", shock("x"), (128, 1, 1), (3, 0, 0), steps=-1, gamma=1.4, bc=dict(x="ic"),
+        riemann_solver="hllc", CFL=0.8, T=0.1, ic_spec=dict(cls="Shock1D", kwargs=dict(dim="x")), **lim)
+    add("rhs", "quad_p3_dirichlet", FourQuadrant(seed=5), (32, 32, 1), (3, 3, 0), gamma=1.4,
+        bc=dict(x=("dirichlet", "outflow"), y=("outflow", "free"), x_value=("inflow_state", None)),
+        riemann_solver="hllc", **lim)
+    add("rhs", "quad_p3_ic_wall", FourQuadrant(seed=6), (32, 40, 1), (3, 3, 0), gamma=1.4,
+        bc=dict(x="ic", y=("outflow", "dirichlet"), y_value=(None, "wall_y_high")), riemann_solver="hllc",
+        ic_spec=dict(cls="FourQuadrant", kwargs=dict(seed=6)), **lim)
+    add("steps", "kh_dirichlet_t", kh((32, 32, 1)), (32, 32, 1), (3, 3, 0), steps=3, gamma=1.4,
+        bc=dict(x="periodic", y="dirichlet", y_value=("wall_y_low", "wall_y_high")), riemann_solver="hllc", **lim)
+    add("rhs", "box3d_dirichlet", Sinus(dims="xyz", vx=0.5, vy=0.25, vz=-0.3), (10, 12, 14), (2, 2, 2),
+        gamma=1.4, bc=dict(x=("dirichlet", "outflow"), y=("reflective", "free"), z=("ic", "dirichlet"),
+                           x_value=("box_x_low", None), z_value=(None, "box_z_high")),
+        riemann_solver="hllc", ic_spec=dict(cls="Sinus", kwargs=dict(dims="xyz", vx=0.5, vy=0.25, vz=-0.3)), **lim)
     return cases
 
 
@@ -176,10 +193,23 @@ def run_case(case, outdir):
     from fvhoe.boundary_conditions import BoundaryCondition
     from fvhoe.solver import EulerSolver
 
+    import bc_values
+
     kw = dict(case["kw"])
     T = kw.pop("T", None)
     passives = kw.pop("passives", False)
+    ic_spec = kw.pop("ic_spec", None)
     bc_kw = kw.pop("bc", None)
+    bc_names = [[None, None], [None, None], [None, None]]
+    if bc_kw is not None:
+        bc_kw = dict(bc_kw)
+        for a, dim in enumerate("xyz"):
+            names = bc_kw.pop(f"{dim}_value", None)
+            if names is None:
+                continue
+            names = names if isinstance(names, tuple) else (names, names)
+            bc_names[a] = list(names)
+            bc_kw[f"{dim}_value"] = tuple(bc_values.resolve(nm) for nm in names)
     nx, ny, nz = case["n"]
     px, py, pz = case["p"]
     domain = kw.pop("domain", ((0, 1), (0, 1), (0, 1)))
@@ -221,6 +251,7 @@ def run_case(case, outdir):
         NAD_vars=list(solver.NAD_vars) if solver.NAD_vars is not None else None,
         PAD=_json_pad(solver.PAD), SED=solver.SED, SED_tolerance=solver.SED_tolerance,
         convex=solver.convex, csq_floor=solver.csq_floor, integrator=case["integrator"],
+        bc_values=bc_names, ic_spec=ic_spec, slab_buffer_size=solver.slab_buffer_size,
     )
     u0 = solver.am.get_numpy("u")
     out = dict(config=np.array(json.dumps(config)), u0=u0)

@@ -165,7 +165,12 @@ def test_boundary_condition_parsing_and_refusals():
     assert bc.x == ("reflective", "outflow") and bc.y == ("free", "free") and bc.z == ("periodic", "periodic")
     assert bc.kinds((True, True, False))[0] == ("reflective", "outflow")
     with pytest.raises(NotImplementedError):
+        BoundaryCondition(y="special-case-double-mach-reflection-y=0").kinds((True, True, False))
+    # Dirichlet sides need a callable or an array of values (the reference raises when it applies them)
+    with pytest.raises(ValueError):
         BoundaryCondition(x="dirichlet").kinds((True, False, False))
+    assert BoundaryCondition(x=("ic", "dirichlet"), x_value=(None, np.ones(5))).kinds((True, False, False))[0] == (
+        "ic", "dirichlet")
     with pytest.raises(ValueError):
         BoundaryCondition(x=("outflow", "periodic")).kinds((True, False, False))
     with pytest.raises(ValueError):
