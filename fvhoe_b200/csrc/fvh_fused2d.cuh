@@ -570,7 +570,19 @@ __device__ __forceinline__ void tile2_detect(const double* __restrict__ ustar, G
   Tc* B = A + D::A;
   const int x0 = by * TX, y0 = bx * TY;
   primitives_tile<Tc, P, OX, OY, KC>(ustar, g, x0 - 3, y0 - 3, A, B, c, t, ph);
-  // A now holds W* on [x0-3, x0+TX+3) x [y0-3, y0+TY+3)
+  // A now holds W* on [x0-3, x0+TX+3) x [y0-3, y0+TY+3); B is free: stage W on
+  // [x0-1, x0+TX+1) x [y0-1, y0+TY+1) there for the 3x3 box extrema
+  constexpr int WX = TX + 2, WY = TY + 2;
+  static_assert(WX * WY * 5 <= D::B, "W tile must fit in the second buffer");
+  Tc* Wt = B;
+  for (int i = threadIdx.x; i < WX * WY; i += blockDim.x) {
+    const int r = i / WY, q = i - r * WY;
+    const int x = min(x0 - 1 + r, g.nx + W.g - 1), y = min(y0 - 1 + q, g.ny + W.g - 1);
+    const Tc* p = W.p + W.at(x, y);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) Wt[(v * WX + r) * WY + q] = p[v * W.vs];
+  }
+  __syncthreads();
   Tc grange[5], glower[5], gupper[5];
 #pragma unroll
   for (int v = 0; v < 5; ++v) {
@@ -588,18 +600,17 @@ __device__ __forceinline__ void tile2_detect(const double* __restrict__ ustar, G
     const int r = i / TY, q = i - r * TY;
     const int x = x0 + r, y = y0 + q;
     if (x >= g.nx || y >= g.ny) continue;
-    const int ow = W.at(x, y);
     bool nad_any = false;
     Tc ind_min = Tc(0), pad_ind = Tc(0);
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
-      const Tc* pw = W.p + v * W.vs + ow;
+      const Tc* pw = Wt + (v * WX + r + 1) * WY + q + 1;
       Tc big = pw[0], small = big;
 #pragma unroll
       for (int a = -1; a <= 1; ++a)
 #pragma unroll
         for (int b = -1; b <= 1; ++b) {
-          const Tc xv = pw[a * W.sx + b];
+          const Tc xv = pw[a * WY + b];
           big = fmax(big, xv);
           small = fmin(small, xv);
         }
