@@ -39,6 +39,7 @@ EXPORTS = (
     "fvh_trouble_flags",
     "fvh_trouble_log",
     "fvh_set_log_mode",
+    "fvh_set_log_divisor",
     "fvh_get_stats",
     "fvh_kernel_launches",
     "fvh_profile_enable",
@@ -168,6 +169,8 @@ def _load():
     lib.fvh_trouble_flags.argtypes = [vp, vp, vp]
     lib.fvh_trouble_log.argtypes = [vp, ctypes.c_double, vp, vp, vp, vp]
     lib.fvh_set_log_mode.argtypes = [vp, ctypes.c_int]
+    lib.fvh_set_log_divisor.argtypes = [vp, ctypes.c_double]
+    lib.fvh_set_log_divisor.restype = ctypes.c_int
     lib.fvh_get_stats.argtypes = [vp, ctypes.POINTER(FvhStats), vp]
     lib.fvh_kernel_launches.argtypes = []
     lib.fvh_kernel_launches.restype = ctypes.c_uint64

@@ -524,10 +524,15 @@ int fvh_step(fvh_handle* h, double* u, int integrator, double t, int has_target,
     c.t = t;
     c.target = target;
     c.log_mode = next_log_mode(h);
+    c.log_div = k == stages - 1 ? h->log_divisor : 0.0;
     const int st = run_stage(h, c, s);
-    if (st) return st;
+    if (st) {
+      h->log_divisor = 0.0;
+      return st;
+    }
     in = h->S[k & 1];
   }
+  h->log_divisor = 0.0;
   return read_dt(h, s, dt_out);
 }
 
@@ -572,6 +577,13 @@ int fvh_trouble_log(fvh_handle* h, double divide_by, double* trouble, double* na
   }
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(h, FVH_ERR_CUDA, cudaGetErrorString(e));
+  return FVH_OK;
+}
+
+int fvh_set_log_divisor(fvh_handle* h, double divisor) {
+  if (!h) return FVH_ERR_ARG;
+  if (!(divisor >= 0.0)) return fail(h, FVH_ERR_ARG, "the divisor must be >= 0");
+  h->log_divisor = divisor;
   return FVH_OK;
 }
 

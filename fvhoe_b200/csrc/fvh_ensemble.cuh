@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(256)
     const f2::V2<const Tc> Wc{(const Tc*)p->W, a.gW, g.ny + 2 * a.gW, (g.nx + 2 * a.gW) * (g.ny + 2 * a.gW)};
     __syncthreads();
     f2::tile2_fluxes<Tc, P, TX, TY, KC, KF>(Wc, stage_input(p, stage), g, f2::make_v2((Tc*)p->F, g.nx + 1, g.ny, 0),
-                                            f2::make_v2((Tc*)p->G, g.nx, g.ny + 1, 0), a.apost ? p->us : nullptr,
+                                            f2::make_v2((Tc*)p->G, g.nx, g.ny + 1, 0), a.apost ? (Tc*)p->us : nullptr,
                                             a.crule, a.trule, a.lrule, a.rrule, a.ph, p->cx, p->cy, dt, nullptr, 1,
                                             a.limiter, li % p->tiles_y[1], li / p->tiles_y[1], smem_raw);
   }
@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(256)
       const f2::Geo g = p->g;
       const f2::V2<const Tc> Wc{(const Tc*)p->W, a.gW, g.ny + 2 * a.gW, (g.nx + 2 * a.gW) * (g.ny + 2 * a.gW)};
       __syncthreads();
-      f2::tile2_detect<Tc, P, TX, TY, KC>(p->us, g, Wc, a.crule, a.trule, a.ph, a.ds, p->sc, p->trouble, nullptr,
+      f2::tile2_detect<Tc, P, TX, TY, KC>((const Tc*)p->us, g, Wc, a.crule, a.trule, a.ph, a.ds, p->sc, p->trouble, nullptr,
                                           nullptr, nullptr, li % p->tiles_y[2], li / p->tiles_y[2], smem_raw);
     }
     if (!grid_barrier(a.bar)) return;

@@ -54,17 +54,18 @@ __host__ __device__ inline V2<T> make_v2(T* p, int nx, int ny, int g) {
   return v;
 }
 
-// Conserved state at a (possibly ghost) cell of the 2D grid. Coordinates of
+// Conserved state at a (possibly ghost) cell of the 2D grid, stored as Tin
+// (double for the state, the compute type for the candidate). Coordinates of
 // tile points that no output needs are clamped into the ghost range first.
-template <typename Tc>
-__device__ __forceinline__ void load_state2(const double* __restrict__ u, const Geo& g, int x, int y, Tc* out) {
+template <typename Tc, typename Tin>
+__device__ __forceinline__ void load_state2(const Tin* __restrict__ u, const Geo& g, int x, int y, Tc* out) {
   x = min(max(x, -g.gmax), g.nx + g.gmax - 1);
   y = min(max(y, -g.gmax), g.ny + g.gmax - 1);
   if (g.slabs) {
     int i[3] = {0, 0, 0};
     i[g.dx] = x;
     i[g.dy] = y;
-    const State5<Tc> s = load_state5_dirichlet<Tc>(u, g.slabs, i[0], i[1], i[2]);
+    const State5<Tc> s = load_state5_dirichlet<Tc, Tin>(u, g.slabs, i[0], i[1], i[2]);
 #pragma unroll
     for (int v = 0; v < 5; ++v) out[v] = s.v[v];
     return;
@@ -76,7 +77,7 @@ __device__ __forceinline__ void load_state2(const double* __restrict__ u, const 
   const int o = jx * g.ny + jy;
 #pragma unroll
   for (int v = 0; v < 5; ++v) {
-    double val = u[v * plane + o];
+    double val = (double)u[v * plane + o];
     if ((v == 1 + g.dx && fx) || (v == 1 + g.dy && fy)) val = -val;
     out[v] = (Tc)val;
   }
@@ -164,8 +165,8 @@ struct PrimsDims {
 
 // W on [x0, x0+OX) x [y0, y0+OY), computed in two shared buffers; the result
 // is left in A as an OX x OY tile. Rules: centre c and transverse t (KC taps).
-template <typename Tc, int P, int OX, int OY, int KC>
-__device__ __forceinline__ void primitives_tile(const double* __restrict__ u, const Geo& g, int x0, int y0, Tc* A,
+template <typename Tc, int P, int OX, int OY, int KC, typename Tin>
+__device__ __forceinline__ void primitives_tile(const Tin* __restrict__ u, const Geo& g, int x0, int y0, Tc* A,
                                                 Tc* B, const Rule<Tc, KC>& c, const Rule<Tc, KC>& t,
                                                 const Phys<Tc>& ph) {
   using D = PrimsDims<P, OX, OY>;
@@ -354,7 +355,7 @@ struct FluxDims {
 
 template <typename Tc, int P, int TX, int TY, int KC, int KF>
 __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __restrict__ u, Geo g, V2<Tc> F, V2<Tc> G,
-                                             double* __restrict__ ustar, Rule<Tc, KC> c, Rule<Tc, KC> t,
+                                             Tc* __restrict__ ustar, Rule<Tc, KC> c, Rule<Tc, KC> t,
                                              Rule<Tc, KF> lrule, Rule<Tc, KF> rrule, Phys<Tc> ph, double cx,
                                              double cy, double dt, const uint8_t* __restrict__ pred, int muscl,
                                              int limiter, int bx, int by, unsigned char* smem_raw) {
@@ -507,7 +508,7 @@ __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __res
       Tc d = Tc(0);
       d = d + (Tc)cx * (FX[(v * (TX + 1) + r + 1) * TY + q] - FX[(v * (TX + 1) + r) * TY + q]);
       d = d + (Tc)cy * (GY[(v * TX + r) * (TY + 1) + q + 1] - GY[(v * TX + r) * (TY + 1) + q]);
-      ustar[v * plane + o] = u[v * plane + o] + dt * (double)d;
+      ustar[v * plane + o] = (Tc)(u[v * plane + o] + dt * (double)d);
     }
   }
   // predicted cells: their faces take the fallback flux now, blended as the
@@ -544,14 +545,33 @@ __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __res
   }
 }
 
+// The stage's time step: dt = CFL h / max speed or the fixed dt
+// (fvhoe/hydro.py:270-294); the first stage of a step also fixes the step's dt,
+// clamped so that t + dt does not pass the target (fvhoe/ode.py:11-22).
+struct DtSpec {
+  double cfl_h, fixed_dt, t, target;
+  int use_fixed, first_stage, has_target, pad_;
+};
+
 template <typename Tc, int P, int TX, int TY, int KC, int KF>
 __global__ void __launch_bounds__(256)
-    k2_fluxes(V2<const Tc> W, const double* __restrict__ u, Geo g, V2<Tc> F, V2<Tc> G, double* __restrict__ ustar,
+    k2_fluxes(V2<const Tc> W, const double* __restrict__ u, Geo g, V2<Tc> F, V2<Tc> G, Tc* __restrict__ ustar,
               Rule<Tc, KC> c, Rule<Tc, KC> t, Rule<Tc, KF> lrule, Rule<Tc, KF> rrule, Phys<Tc> ph, double cx,
-              double cy, const Scalars* __restrict__ sc, const uint8_t* __restrict__ pred, int muscl, int limiter) {
+              double cy, Scalars* __restrict__ sc, DtSpec dts, const uint8_t* __restrict__ pred, int muscl,
+              int limiter) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  tile2_fluxes<Tc, P, TX, TY, KC, KF>(W, u, g, F, G, ustar, c, t, lrule, rrule, ph, cx, cy, sc->dt_stage, pred, muscl,
-                                      limiter, blockIdx.x, blockIdx.y, smem_raw);
+  // every block derives dt from the reduced CFL key; block (0, 0) publishes it
+  const double dt = dts.use_fixed ? dts.fixed_dt : dts.cfl_h / key_value(sc->cfl_key);
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+    sc->dt_stage = dt;
+    if (dts.first_stage) {
+      double d = dt;
+      if (dts.has_target && dts.target - dts.t < d) d = dts.target - dts.t;
+      sc->dt_step = d;
+    }
+  }
+  tile2_fluxes<Tc, P, TX, TY, KC, KF>(W, u, g, F, G, ustar, c, t, lrule, rrule, ph, cx, cy, dt, pred, muscl, limiter,
+                                      blockIdx.x, blockIdx.y, smem_raw);
 }
 
 // ---------------------------------------------------------------------------
@@ -559,7 +579,7 @@ __global__ void __launch_bounds__(256)
 // tile's cells against W (global, >= 3 ghosts).
 // ---------------------------------------------------------------------------
 template <typename Tc, int P, int TX, int TY, int KC>
-__device__ __forceinline__ void tile2_detect(const double* __restrict__ ustar, Geo g, V2<const Tc> W, Rule<Tc, KC> c,
+__device__ __forceinline__ void tile2_detect(const Tc* __restrict__ ustar, Geo g, V2<const Tc> W, Rule<Tc, KC> c,
                                              Rule<Tc, KC> t, Phys<Tc> ph, DetectSpec ds, Scalars* __restrict__ sc,
                                              uint8_t* __restrict__ trouble, double* __restrict__ log_trouble,
                                              double* __restrict__ log_nad, double* __restrict__ log_pad, int bx,
@@ -659,15 +679,7 @@ __device__ __forceinline__ void tile2_detect(const double* __restrict__ ustar, G
       const double lt = tr ? 1.0 : 0.0;
       const double ln = nad_any ? -(double)ind_min : 0.0;
       const double lp = pad_trouble ? -(double)pad_ind : 0.0;
-      if (ds.log_mode == 1) {
-        log_trouble[o] = lt;
-        log_nad[o] = ln;
-        log_pad[o] = lp;
-      } else {
-        log_trouble[o] = log_trouble[o] + lt;
-        log_nad[o] = log_nad[o] + ln;
-        log_pad[o] = log_pad[o] + lp;
-      }
+      log_write(ds, o, lt, ln, lp, log_trouble, log_nad, log_pad);
     }
   }
   block_count_add(count, &sc->troubled);
@@ -675,7 +687,7 @@ __device__ __forceinline__ void tile2_detect(const double* __restrict__ ustar, G
 
 template <typename Tc, int P, int TX, int TY, int KC>
 __global__ void __launch_bounds__(256)
-    k2_detect(const double* __restrict__ ustar, Geo g, V2<const Tc> W, Rule<Tc, KC> c, Rule<Tc, KC> t, Phys<Tc> ph,
+    k2_detect(const Tc* __restrict__ ustar, Geo g, V2<const Tc> W, Rule<Tc, KC> c, Rule<Tc, KC> t, Phys<Tc> ph,
               DetectSpec ds, Scalars* __restrict__ sc, uint8_t* __restrict__ trouble, double* __restrict__ log_trouble,
               double* __restrict__ log_nad, double* __restrict__ log_pad) {
   extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -53,6 +53,7 @@ struct fvh_handle {
   bool last_stage_fused = false;  // the last stage ran the fused 2D kernels
 
   int log_mode_next = 1;          // log mode of the next stage
+  double log_divisor = 0.0;       // divisor applied by the next step's last stage (one-shot)
   fvh::Profiler* prof = nullptr;  // per-launch timing, when enabled
   fvh::KernelTotals prof_totals{};
   std::string err;
@@ -68,6 +69,7 @@ struct StageCall {
   double t;
   double target;
   int log_mode;            // 0 none, 1 overwrite, 2 add
+  double log_div;          // > 0: divide the trouble-log sums by it after this stage
 };
 
 // Runs one stage on the stream; returns an FVH_ status.

@@ -168,8 +168,8 @@ __device__ __forceinline__ int state_stride(const Grid& g, int axis) {
 // side returns its slab value at the coordinates mapped so far; a mirrored,
 // periodic or free side maps its coordinate into the interior (the reflective
 // sign flips apply to whatever value ends up copied).
-template <typename Tc>
-__device__ __forceinline__ void dirichlet_core(const double* __restrict__ u, const Slabs* __restrict__ sl, int nv,
+template <typename Tc, typename Tin>
+__device__ __forceinline__ void dirichlet_core(const Tin* __restrict__ u, const Slabs* __restrict__ sl, int nv,
                                                int i0, int i1, int i2, Tc* out) {
   int i[3] = {i0, i1, i2};
   bool flip[3] = {false, false, false};
@@ -201,7 +201,7 @@ __device__ __forceinline__ void dirichlet_core(const double* __restrict__ u, con
   const int plane = sl->n[0] * sl->n[1] * sl->n[2];
   const int o = (i[0] * sl->n[1] + i[1]) * sl->n[2] + i[2];
   for (int v = 0; v < nv; ++v) {
-    double x = u[v * plane + o];
+    double x = (double)u[v * plane + o];
     if ((v == 1 && flip[0]) || (v == 2 && flip[1]) || (v == 3 && flip[2])) x = -x;
     out[v] = (Tc)x;
   }
@@ -213,7 +213,7 @@ __device__ __forceinline__ void dirichlet_core(const double* __restrict__ u, con
 template <typename Tc>
 __device__ __noinline__ void load_state_dirichlet(const double* __restrict__ u, const Slabs* __restrict__ sl, int nv,
                                                   int i0, int i1, int i2, Tc* out) {
-  dirichlet_core<Tc>(u, sl, nv, i0, i1, i2, out);
+  dirichlet_core<Tc, double>(u, sl, nv, i0, i1, i2, out);
 }
 
 template <typename Tc>
@@ -221,11 +221,11 @@ struct State5 {
   Tc v[5];
 };
 
-template <typename Tc>
-__device__ __noinline__ State5<Tc> load_state5_dirichlet(const double* __restrict__ u, const Slabs* __restrict__ sl,
+template <typename Tc, typename Tin>
+__device__ __noinline__ State5<Tc> load_state5_dirichlet(const Tin* __restrict__ u, const Slabs* __restrict__ sl,
                                                          int i0, int i1, int i2) {
   State5<Tc> s;
-  dirichlet_core<Tc>(u, sl, 5, i0, i1, i2, s.v);
+  dirichlet_core<Tc, Tin>(u, sl, 5, i0, i1, i2, s.v);
   return s;
 }
 
@@ -589,7 +589,31 @@ struct DetectSpec {
   int force_trouble;
   int axes[3];   // the active axes, ascending
   int log_mode;  // 0: no logging, 1: overwrite the running sums, 2: add to them
+  double log_div;  // > 0: divide the sums by it afterwards (the step's last stage)
 };
+
+// Running trouble / NAD / PAD sums of log_troubles (fvhoe/solver.py:794-833):
+// mode 1 overwrites them, mode 2 adds this stage's values; a positive log_div
+// then divides them, the reset branch of log_troubles (:809-820) done here
+// instead of in a separate pass over the arrays.
+__device__ __forceinline__ void log_write(const DetectSpec& ds, int o, double lt, double ln, double lp,
+                                          double* __restrict__ log_trouble, double* __restrict__ log_nad,
+                                          double* __restrict__ log_pad) {
+  double a = lt, b = ln, c = lp;
+  if (ds.log_mode == 2) {
+    a = log_trouble[o] + lt;
+    b = log_nad[o] + ln;
+    c = log_pad[o] + lp;
+  }
+  if (ds.log_div > 0.0) {
+    a = a / ds.log_div;
+    b = b / ds.log_div;
+    c = c / ds.log_div;
+  }
+  log_trouble[o] = a;
+  log_nad[o] = b;
+  log_pad[o] = c;
+}
 
 // Whether the smooth-extrema detector's alpha along one line is below 1
 // (fvhoe/smooth_extrema_detection.py:8-50). a[0..6] are the values at
@@ -717,15 +741,7 @@ __global__ void __launch_bounds__(256)
       const double lt = t ? 1.0 : 0.0;
       const double ln = nad_any ? -(double)ind_min : 0.0;
       const double lp = pad_trouble ? -(double)pad_ind : 0.0;
-      if (ds.log_mode == 1) {
-        log_trouble[o] = lt;
-        log_nad[o] = ln;
-        log_pad[o] = lp;
-      } else {
-        log_trouble[o] = log_trouble[o] + lt;
-        log_nad[o] = log_nad[o] + ln;
-        log_pad[o] = log_pad[o] + lp;
-      }
+      log_write(ds, o, lt, ln, lp, log_trouble, log_nad, log_pad);
     }
   }
   block_count_add(count, &sc->troubled);

@@ -464,6 +464,7 @@ int run_stage_t(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     for (int a = 0; a < 3; ++a)
       if (h->active[a]) ds.axes[na++] = a;
     ds.log_mode = cfg.log_troubles ? c.log_mode : 0;
+    ds.log_div = ds.log_mode ? c.log_div : 0.0;
     {
       const double log_bytes = ds.log_mode ? 3.0 * (ds.log_mode == 2 ? 2 : 1) * region_bytes(rint, 1, 8) : 0.0;
       LaunchScope scope(KK_DETECT,
@@ -540,7 +541,7 @@ template <typename Tc>
 struct FusedTiles;
 template <>
 struct FusedTiles<float> {
-  static constexpr int PX = 16, PY = 32;  // primitives
+  static constexpr int PX = 32, PY = 32;  // primitives (register-limited to 3 blocks/SM either way)
   static constexpr int FX = 16, FY = 32;  // fluxes
   static constexpr int DX = 16, DY = 32;  // detection
   static constexpr int EX = 16, EY = 32;  // fallback + final
@@ -619,11 +620,15 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
                                  h->sc);
   }
   if ((st = set_cuda_error(h, "fused primitives"))) return st;
-  {
-    LaunchScope scope(KK_SMALL, 0.0, s);
-    k_finalize_dt<<<1, 1, 0, s>>>(h->sc, h->cfl_h, cfg.use_fixed_dt, cfg.fixed_dt, c.first_stage, c.has_target,
-                                  c.t, c.target);
-  }
+  // the stage's dt is derived (and published) by the flux kernel
+  f2::DtSpec dts{};
+  dts.cfl_h = h->cfl_h;
+  dts.fixed_dt = cfg.fixed_dt;
+  dts.t = c.t;
+  dts.target = c.target;
+  dts.use_fixed = cfg.use_fixed_dt;
+  dts.first_stage = c.first_stage;
+  dts.has_target = c.has_target;
   // learned predictor: flags from W and the extrema just reduced
   const uint8_t* pred = nullptr;
   if (h->mlp && apost) {
@@ -639,10 +644,11 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     auto kern = f2::k2_fluxes<Tc, P, T::FX, T::FY, KC, KF>;
     set_smem((const void*)kern, smem);
     const dim3 grid((g.ny + T::FY - 1) / T::FY, (g.nx + T::FX - 1) / T::FX);
-    LaunchScope scope(KK_FACE, cells * 5 * (3.0 * sizeof(Tc) + (apost ? 16.0 : 0.0)), s);
+    // W in, F and G out; with limiting, the state in and the candidate (compute type) out
+    LaunchScope scope(KK_FACE, cells * 5 * (3.0 * sizeof(Tc) + (apost ? 8.0 + sizeof(Tc) : 0.0)), s);
     f2::V2<const Tc> Wc{(const Tc*)h->W, h->gW, g.ny + 2 * h->gW, (g.nx + 2 * h->gW) * (g.ny + 2 * h->gW)};
-    kern<<<grid, 256, smem, s>>>(Wc, c.stage_in, g, F, G, apost ? h->Us : nullptr, crule, trule, lrule, rrule, ph,
-                                 cx, cy, h->sc, pred, 1, cfg.slope_limiter);
+    kern<<<grid, 256, smem, s>>>(Wc, c.stage_in, g, F, G, apost ? (Tc*)h->Us : nullptr, crule, trule, lrule, rrule, ph,
+                                 cx, cy, h->sc, dts, pred, 1, cfg.slope_limiter);
   }
   if ((st = set_cuda_error(h, "fused fluxes"))) return st;
   // 3. W* + detection
@@ -659,14 +665,16 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     ds.pad_hi = cfg.pad_hi;
     ds.force_trouble = cfg.force_trouble;
     ds.log_mode = cfg.log_troubles ? c.log_mode : 0;
+    ds.log_div = ds.log_mode ? c.log_div : 0.0;
     using D = f2::PrimsDims<P, T::DX + 6, T::DY + 6>;
     const size_t smem = (size_t)(D::A + D::B) * sizeof(Tc);
     auto kern = f2::k2_detect<Tc, P, T::DX, T::DY, KC>;
     set_smem((const void*)kern, smem);
     const dim3 grid((g.ny + T::DY - 1) / T::DY, (g.nx + T::DX - 1) / T::DX);
-    LaunchScope scope(KK_DETECT, cells * (5 * 8.0 + 5 * sizeof(Tc) + 1 + (ds.log_mode ? 48.0 : 0.0)), s);
+    // candidate and W in (compute type), flags out, trouble-log sums in and out
+    LaunchScope scope(KK_DETECT, cells * (10.0 * sizeof(Tc) + 1 + (ds.log_mode ? 48.0 : 0.0)), s);
     f2::V2<const Tc> Wc{(const Tc*)h->W, h->gW, g.ny + 2 * h->gW, (g.nx + 2 * h->gW) * (g.ny + 2 * h->gW)};
-    kern<<<grid, 256, smem, s>>>(h->Us, g, Wc, crule, trule, ph, ds, h->sc, h->trouble, h->logs[0], h->logs[1],
+    kern<<<grid, 256, smem, s>>>((const Tc*)h->Us, g, Wc, crule, trule, ph, ds, h->sc, h->trouble, h->logs[0], h->logs[1],
                                  h->logs[2]);
     if ((st = set_cuda_error(h, "fused detect"))) return st;
   }

@@ -461,6 +461,11 @@ class EulerSolver(ODE):
         dt = ctypes.c_double()
         self._upload_boundaries()
         self._set_log_mode()
+        if self._log_enabled:
+            # the division step_helper_function would apply after this step, done by the step's last stage
+            self._capi.check(self._capi.lib.fvh_set_log_divisor(
+                self._handle, float(self.trouble_counter + _STAGES[integrator])), self._handle)
+            self._logs_divided = True
         self._capi.check(
             self._capi.lib.fvh_step(
                 self._handle, ctypes.c_void_p(u.data_ptr()), self._capi.INTEGRATOR[integrator], float(self.t),
@@ -477,11 +482,13 @@ class EulerSolver(ODE):
     def step_helper_function(self):
         # log_troubles(reset=True) of fvhoe/solver.py:809-820
         if self._log_enabled and self.trouble_counter > 0:
-            self._capi.check(
-                self._capi.lib.fvh_trouble_log(self._handle, float(self.trouble_counter), None, None, None,
-                                               self._stream()),
-                self._handle,
-            )
+            if not getattr(self, "_logs_divided", False):
+                self._capi.check(
+                    self._capi.lib.fvh_trouble_log(self._handle, float(self.trouble_counter), None, None, None,
+                                                   self._stream()),
+                    self._handle,
+                )
+            self._logs_divided = False
             self.trouble_counter = 0
 
     def trouble_flags(self) -> np.ndarray:

@@ -202,6 +202,13 @@ int fvh_trouble_log(fvh_handle* h, double divide_by, double* trouble, double* na
  * 2 adds to them (the two branches of log_troubles, fvhoe/solver.py:821-833). */
 int fvh_set_log_mode(fvh_handle* h, int mode);
 
+/* Makes the last stage of the next fvh_step divide the running sums by
+ * divisor after adding its values: the reset branch of log_troubles
+ * (fvhoe/solver.py:809-820) that the reference runs after every step, done in
+ * the detection pass instead of in a separate one (fvh_trouble_log with
+ * divide_by). 0 = no division. Applies to one fvh_step. */
+int fvh_set_log_divisor(fvh_handle* h, double divisor);
+
 /* Statistics of the last stage; synchronises the stream. */
 int fvh_get_stats(fvh_handle* h, fvh_stats* out, void* stream);
 

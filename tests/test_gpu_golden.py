@@ -112,3 +112,33 @@ def test_fused2d_fp32_close_to_generic_fp32(p):
     diff = (ka - kb).abs().max().item()
     scale = kb.abs().max().item()
     assert diff <= 1e-4 * scale, (diff, scale)
+
+
+def test_log_division_in_the_last_stage_equals_the_separate_pass():
+    """fvh_set_log_divisor makes the step's last stage divide the trouble-log sums
+    (the reset branch of log_troubles); the result equals the separate division."""
+    import ctypes
+
+    import torch
+
+    from fvhoe_b200 import EulerSolver, KelvinHelmholtzNoise2D, _capi
+
+    kw = dict(w0=KelvinHelmholtzNoise2D(n=(48, 48), seed=5), nx=48, ny=48, px=3, py=3, gamma=1.4,
+              a_posteriori_slope_limiting=True, NAD=1e-5, progress_bar=False)
+    logs = []
+    for fused in (True, False):
+        s = EulerSolver(**kw)
+        h, lib = s._handle, _capi.lib
+        u = ctypes.c_void_p(s.am("u").data_ptr())
+        for k in range(3):
+            _capi.check(lib.fvh_set_log_mode(h, 1 if k else 2), h)
+            if fused:
+                _capi.check(lib.fvh_set_log_divisor(h, 4.0 if k == 0 else 3.0), h)
+            _capi.check(lib.fvh_step(h, u, _capi.INTEGRATOR["ssprk3"], 0.0, 0, 0.0, None, None), h)
+            if not fused:
+                _capi.check(lib.fvh_trouble_log(h, 4.0 if k == 0 else 3.0, None, None, None, None), h)
+        torch.cuda.synchronize()
+        logs.append([x.copy() for x in s._trouble_logs()])
+    for a, b in zip(*logs):
+        assert np.array_equal(a, b)
+    assert logs[0][0].max() > 0
