@@ -140,7 +140,7 @@ struct Smem {
   using DD = f2::PrimsDims<P, TX + 6, TY + 6>;
   using DE = f2::FinalDims<TX, TY>;
   static constexpr int prim = (DP::A + DP::B) * (int)sizeof(Tc);
-  static constexpr int flux = (DF::SW + DF::SA + DF::SB + DF::SF + DF::SG) * (int)sizeof(Tc);
+  static constexpr int flux = DF::TOTAL * (int)sizeof(Tc);
   static constexpr int detect = (DD::A + DD::B) * (int)sizeof(Tc);
   static constexpr int fin = (DE::SP + DE::SF + DE::SG) * (int)sizeof(Tc);
   static constexpr int bytes = f2::Max<f2::Max<prim, flux>::value, f2::Max<detect, fin>::value>::value;

@@ -150,6 +150,101 @@ struct Max {
   static constexpr int value = a > b ? a : b;
 };
 
+__host__ __device__ constexpr int up4(int n) { return (n + 3) / 4 * 4; }
+
+// N (1, 2 or 4) consecutive elements at an address aligned to N elements, in
+// as few 8- or 16-byte accesses as the type allows.
+template <int N>
+__device__ __forceinline__ void ldn(const float* p, float* o) {
+  if constexpr (N == 4) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    o[0] = t.x, o[1] = t.y, o[2] = t.z, o[3] = t.w;
+  } else if constexpr (N == 2) {
+    const float2 t = *reinterpret_cast<const float2*>(p);
+    o[0] = t.x, o[1] = t.y;
+  } else {
+    o[0] = p[0];
+  }
+}
+template <int N>
+__device__ __forceinline__ void ldn(const double* p, double* o) {
+  if constexpr (N == 1) {
+    o[0] = p[0];
+  } else {
+#pragma unroll
+    for (int a = 0; a < N; a += 2) {
+      const double2 t = *reinterpret_cast<const double2*>(p + a);
+      o[a] = t.x, o[a + 1] = t.y;
+    }
+  }
+}
+template <int N>
+__device__ __forceinline__ void stn(float* p, const float* o) {
+  if constexpr (N == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4(o[0], o[1], o[2], o[3]);
+  } else if constexpr (N == 2) {
+    *reinterpret_cast<float2*>(p) = make_float2(o[0], o[1]);
+  } else {
+    p[0] = o[0];
+  }
+}
+template <int N>
+__device__ __forceinline__ void stn(double* p, const double* o) {
+  if constexpr (N == 1) {
+    p[0] = o[0];
+  } else {
+#pragma unroll
+    for (int a = 0; a < N; a += 2) *reinterpret_cast<double2*>(p + a) = make_double2(o[a], o[a + 1]);
+  }
+}
+
+// One stencil sweep over the five variable planes of a shared tile, four
+// consecutive outputs of a row per thread:
+//   out(v, r, q) = sum_k w[k] in(v, r + k AR, OFF + q + k (1 - AR)),  r < NR, q < 4 NG,
+// each sum accumulated from k = 0 upwards as a one-output loop accumulates it,
+// so every output is rounded exactly as before. AR = 1 puts the taps along the
+// strided axis (one aligned vector, or two when OFF is not a multiple of 4, per
+// tap), AR = 0 along the contiguous axis (one window of vectors per output
+// group). Row strides IS/OS and variable strides IVS/OVS are multiples of 4;
+// outputs past the caller's column count land in the padding of the output
+// rows. IN_LIM / OUT_LIM bound the elements the sweep may touch from `in` /
+// `out`. epi(v, r, q, acc) stores the four sums.
+template <typename Tc, int K, int AR, int OFF, int NR, int NG, int IS, int IVS, int IN_LIM, typename Epi>
+__device__ __forceinline__ void sweep4(const Tc* __restrict__ in, const Tc* __restrict__ w, Epi epi) {
+  constexpr int S = OFF & 3, B0 = OFF - S;
+  constexpr int NW = AR ? (S + 7) / 4 : (S + K + 6) / 4;
+  static_assert(IS % 4 == 0 && IVS % 4 == 0, "rows and planes must hold whole vectors");
+  static_assert(4 * IVS + (NR - 1 + (AR ? K - 1 : 0)) * IS + B0 + 4 * (NG - 1) + 4 * NW <= IN_LIM,
+                "sweep reads past its shared region");
+  for (int i = threadIdx.x; i < NR * NG; i += blockDim.x) {
+    const int r = i / NG, q = (i - r * NG) * 4;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const Tc* src = in + v * IVS + r * IS + B0 + q;
+      Tc acc[4] = {Tc(0), Tc(0), Tc(0), Tc(0)};
+      if constexpr (AR) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          Tc x[4 * NW];
+#pragma unroll
+          for (int n = 0; n < NW; ++n) ldn<4>(src + k * IS + 4 * n, x + 4 * n);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[j] = acc[j] + w[k] * x[S + j];
+        }
+      } else {
+        Tc x[4 * NW];
+#pragma unroll
+        for (int n = 0; n < NW; ++n) ldn<4>(src + 4 * n, x + 4 * n);
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[j] = acc[j] + w[k] * x[S + j + k];
+      }
+      epi(v, r, q, acc);
+    }
+  }
+}
+
 // Tile dimensions of the primitive computation producing OX x OY outputs
 // with degree P (centre / transverse rules of radius RC = P / 2).
 template <int P, int OX, int OY>
@@ -332,190 +427,225 @@ __global__ void __launch_bounds__(256)
 // k2_fluxes: high-order X- and Y-face fluxes of a TX x TY cell tile, and the
 // candidate u* = u + dt L(F) of its cells.
 // ---------------------------------------------------------------------------
+// Shared memory of the flux tile: three regions, each reused once its tile is
+// consumed, with rows padded to whole 16-byte vectors (4 elements):
+//   region 0: W tile -> X-face Riemann fluxes -> Y-face Riemann fluxes (-> pointwise tile)
+//   region 1: X centre sweep -> X face fluxes FX
+//   region 2: Y centre sweep -> Y face fluxes GY
 template <int P, int TX, int TY>
 struct FluxDims {
+  static_assert(TY % 4 == 0, "tile columns must hold whole vectors");
   static constexpr int R = (P + 1) / 2;  // face-rule radius
   static constexpr int RC = P / 2;       // centre / transverse radius
   static constexpr int KF = 2 * R + 1;
   static constexpr int H = Max<R + 1, 2 * RC>::value;  // W halo
-  static constexpr int WX = TX + 2 * H, WY = TY + 2 * H;
+  static constexpr int HY = up4(H);                    // W halo on the low Y side (aligned rows)
+  static constexpr int WX = TX + 2 * H, WYS = up4(HY + TY + H);
   // X faces: centre sweep along Y on rows [x0-1-R, x0+TX+R], cols [y0-RC, y0+TY+RC)
-  static constexpr int AXR = TX + 2 * R + 2, AXC = TY + 2 * RC;
-  // Riemann fluxes at faces x0..x0+TX on those cols
-  static constexpr int BXR = TX + 1, BXC = TY + 2 * RC;
+  static constexpr int AXR = TX + 2 * R + 2, AXC = TY + 2 * RC, AXS = up4(AXC);
+  // Riemann fluxes at faces x0..x0+TX on those cols (row stride AXS)
+  static constexpr int BXR = TX + 1;
   // Y faces: centre sweep along X on rows [x0-RC, x0+TX+RC), cols [y0-1-R, y0+TY+R]
-  static constexpr int AYR = TX + 2 * RC, AYC = TY + 2 * R + 2;
-  static constexpr int BYR = TX + 2 * RC, BYC = TY + 1;
-  static constexpr int SW = WX * WY * 5;
-  static constexpr int SA = Max<AXR * AXC, AYR * AYC>::value * 5;
-  static constexpr int SB = Max<BXR * BXC, BYR * BYC>::value * 5;
-  static constexpr int SF = (TX + 1) * TY * 5;
-  static constexpr int SG = TX * (TY + 1) * 5;
+  static constexpr int AYR = TX + 2 * RC, AYC = TY + 2 * R + 2, AYS = up4(AYC);
+  // Riemann fluxes at faces y0..y0+TY of those rows; the Y face fluxes GY (TX rows)
+  static constexpr int BYR = TX + 2 * RC, BYS = up4(TY + 1), GYS = up4(TY + 1);
+  static constexpr int PAD = 16;  // slack after each region for reads that feed padding outputs
+  static constexpr int S0 =
+      Max<Max<WX * WYS, BXR * AXS>::value, Max<BYR * BYS, (TX + 4) * (TY + 4)>::value>::value * 5 + PAD;
+  static constexpr int S1 = Max<AXR * AXS, (TX + 1) * TY>::value * 5 + PAD;
+  static constexpr int S2 = Max<AYR * AYS, TX * GYS>::value * 5 + PAD;
+  static constexpr int TOTAL = S0 + S1 + S2;  // elements of the compute type
 };
 
-template <typename Tc, int P, int TX, int TY, int KC, int KF>
+#ifndef FVH_FLUX_FW
+#define FVH_FLUX_FW 2
+#endif
+// FW: faces per thread in the Riemann phases (1, 2 or 4)
+template <typename Tc, int P, int TX, int TY, int KC, int KF, int FW = FVH_FLUX_FW>
 __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __restrict__ u, Geo g, V2<Tc> F, V2<Tc> G,
                                              Tc* __restrict__ ustar, Rule<Tc, KC> c, Rule<Tc, KC> t,
                                              Rule<Tc, KF> lrule, Rule<Tc, KF> rrule, Phys<Tc> ph, double cx,
                                              double cy, double dt, const uint8_t* __restrict__ pred, int muscl,
                                              int limiter, int bx, int by, unsigned char* smem_raw) {
   using D = FluxDims<P, TX, TY>;
-  constexpr int R = D::R, RC = D::RC, H = D::H;
-  Tc* Ws = reinterpret_cast<Tc*>(smem_raw);
-  Tc* A = Ws + D::SW;
-  Tc* B = A + D::SA;
-  Tc* FX = B + D::SB;
-  Tc* GY = FX + D::SF;
+  constexpr int R = D::R, RC = D::RC, H = D::H, HY = D::HY;
+  Tc* const S0 = reinterpret_cast<Tc*>(smem_raw);
+  Tc* const S1 = S0 + D::S0;
+  Tc* const S2 = S1 + D::S1;
+  Tc* const Ws = S0;  // W tile, WX x WYS: element (r, c) is W(x0-H+r, y0-HY+c)
+  Tc* const AX = S1;  // X centre sweep, AXR x AXS
+  Tc* const AY = S2;  // Y centre sweep, AYR x AYS
+  Tc* const BX = S0;  // X-face Riemann fluxes, BXR x AXS
+  Tc* const FX = S1;  // X face fluxes, (TX+1) x TY
+  Tc* const BY = S0;  // Y-face Riemann fluxes, BYR x BYS
+  Tc* const GY = S2;  // Y face fluxes, TX x GYS
   const int nt = blockDim.x;
   const int x0 = by * TX, y0 = bx * TY;
-  // W tile with H ghosts (W holds gW >= H ghosts)
-  for (int i = threadIdx.x; i < D::WX * D::WY; i += nt) {
-    const int r = i / D::WY, q = i - r * D::WY;
-    const int x = min(x0 - H + r, g.nx + W.g - 1), y = min(y0 - H + q, g.ny + W.g - 1);
-    const Tc* p = W.p + W.at(x, y);
+  // W tile (W holds gW >= H ghosts; points that no output needs are clamped
+  // into range), four columns per access where W's rows are 16-byte aligned
+  {
+    constexpr int NG = D::WYS / 4;
+    const bool vec = ((W.g | W.sx | W.vs) & 3) == 0 && (reinterpret_cast<uintptr_t>(W.p) & 15) == 0;
+    for (int i = threadIdx.x; i < D::WX * NG; i += nt) {
+      const int r = i / NG, cq = (i - r * NG) * 4;
+      const int x = min(max(x0 - H + r, -W.g), g.nx + W.g - 1), y = y0 - HY + cq;
+      Tc val[5][4];
+      if (vec && y >= -W.g && y + 3 <= g.ny + W.g - 1) {
+        const Tc* p = W.p + W.at(x, y);
 #pragma unroll
-    for (int v = 0; v < 5; ++v) Ws[(v * D::WX + r) * D::WY + q] = p[v * W.vs];
-  }
-  __syncthreads();
-  // ---- X faces
-  // centre sweep along Y: A(r, q) at (x0-1-R+r, y0-RC+q)
-  for (int i = threadIdx.x; i < D::AXR * D::AXC; i += nt) {
-    const int r = i / D::AXC, q = i - r * D::AXC;
-    const int wr = r + (H - 1 - R), wq = q + (H - RC) - RC;
+        for (int v = 0; v < 5; ++v) ldn<4>(p + v * W.vs, val[v]);
+      } else {
 #pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      Tc acc = Tc(0);
+        for (int j = 0; j < 4; ++j) {
+          const Tc* p = W.p + W.at(x, min(max(y + j, -W.g), g.ny + W.g - 1));
 #pragma unroll
-      for (int k = 0; k < KC; ++k) acc = acc + c.w[k] * Ws[(v * D::WX + wr) * D::WY + wq + k];
-      A[(v * D::AXR + r) * D::AXC + q] = acc;
+          for (int v = 0; v < 5; ++v) val[v][j] = p[v * W.vs];
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < 5; ++v) stn<4>(Ws + (v * D::WX + r) * D::WYS + cq, val[v]);
     }
   }
   __syncthreads();
-  // face f (x = x0+f) between cells x0+f-1 and x0+f; A row of cell x is x - (x0-1-R)
-  for (int i = threadIdx.x; i < D::BXR * D::BXC; i += nt) {
-    const int f = i / D::BXC, q = i - f * D::BXC;
-    Tc wl[5], wr[5];
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      wl[v] = Tc(0);
-      wr[v] = Tc(0);
-    }
-#pragma unroll
-    for (int k = 0; k < KF; ++k) {
-      const int ra = f + k;      // cell x0+f-1, taps -R..R -> rows f .. f+2R
-      const int rb = f + 1 + k;  // cell x0+f
+  // centre sweeps of both directions from the W tile
+  // X faces: AX(r, q) at (x0-1-R+r, y0-RC+q), taps along Y
+  sweep4<Tc, KC, 0, HY - 2 * RC, D::AXR, D::AXS / 4, D::WYS, D::WX * D::WYS, D::S0 - (H - 1 - R) * D::WYS>(
+      Ws + (H - 1 - R) * D::WYS, c.w,
+      [&](int v, int r, int q, const Tc* acc) { stn<4>(AX + (v * D::AXR + r) * D::AXS + q, acc); });
+  // Y faces: AY(r, q) at (x0-RC+r, y0-1-R+q), taps along X
+  sweep4<Tc, KC, 1, HY - 1 - R, D::AYR, D::AYS / 4, D::WYS, D::WX * D::WYS, D::S0 - (H - 2 * RC) * D::WYS>(
+      Ws + (H - 2 * RC) * D::WYS, c.w,
+      [&](int v, int r, int q, const Tc* acc) { stn<4>(AY + (v * D::AYR + r) * D::AYS + q, acc); });
+  __syncthreads();
+  // ---- X faces: face f (x = x0+f) between cells x0+f-1 and x0+f; AX row of
+  // cell x is x - (x0-1-R). FW consecutive columns per thread.
+  {
+    constexpr int NGF = (D::AXC + FW - 1) / FW;
+    for (int i = threadIdx.x; i < D::BXR * NGF; i += nt) {
+      const int f = i / NGF, q = (i - f * NGF) * FW;
+      Tc wl[FW][5], wr[FW][5];
 #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        wl[v] = wl[v] + rrule.w[k] * A[(v * D::AXR + ra) * D::AXC + q];
-        wr[v] = wr[v] + lrule.w[k] * A[(v * D::AXR + rb) * D::AXC + q];
+#pragma unroll
+        for (int j = 0; j < FW; ++j) wl[j][v] = wr[j][v] = Tc(0);
+#pragma unroll
+        for (int k = 0; k <= KF; ++k) {  // row f+k: tap k of the left cell, tap k-1 of the right
+          Tc x[FW];
+          ldn<FW>(AX + (v * D::AXR + f + k) * D::AXS + q, x);
+#pragma unroll
+          for (int j = 0; j < FW; ++j) {
+            if (k < KF) wl[j][v] = wl[j][v] + rrule.w[k] * x[j];
+            if (k > 0) wr[j][v] = wr[j][v] + lrule.w[k - 1] * x[j];
+          }
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < FW; ++j) {
+        Tc fl[5];
+        riemann_flux<5>(ph, 5, wl[j], wr[j], g.dx, fl);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) BX[(v * D::BXR + f) * D::AXS + q + j] = fl[v];
       }
     }
-    Tc fl[5];
-    riemann_flux<5>(ph, 5, wl, wr, g.dx, fl);
-#pragma unroll
-    for (int v = 0; v < 5; ++v) B[(v * D::BXR + f) * D::BXC + q] = fl[v];
   }
   __syncthreads();
-  // transverse sweep along Y -> FX (TX+1) x TY
-  for (int i = threadIdx.x; i < (TX + 1) * TY; i += nt) {
-    const int f = i / TY, q = i - f * TY;
-    const int x = x0 + f, y = y0 + q;
-    Tc val[5];
+  // X face fluxes: transverse sweep along Y -> FX and F (owned faces)
+  sweep4<Tc, KC, 0, 0, D::BXR, TY / 4, D::AXS, D::BXR * D::AXS, D::S0>(
+      BX, t.w, [&](int v, int f, int q, const Tc* acc) {
+        stn<4>(FX + (v * (TX + 1) + f) * TY + q, acc);
+        const int x = x0 + f;
+        if ((f < TX || x == g.nx) && x <= g.nx) {
+          Tc* o = F.p + F.at(x, y0 + q) + v * F.vs;
 #pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      Tc acc = Tc(0);
-#pragma unroll
-      for (int k = 0; k < KC; ++k) acc = acc + t.w[k] * B[(v * D::BXR + f) * D::BXC + q + k];
-      val[v] = acc;
-      FX[(v * (TX + 1) + f) * TY + q] = acc;
-    }
-    const bool owned = (f < TX || x == g.nx) && x <= g.nx && y < g.ny;
-    if (owned) {
-      Tc* o = F.p + F.at(x, y);
-#pragma unroll
-      for (int v = 0; v < 5; ++v) o[v * F.vs] = val[v];
-    }
-  }
+          for (int j = 0; j < 4; ++j)
+            if (y0 + q + j < g.ny) o[j] = acc[j];
+        }
+      });
   __syncthreads();
-  // ---- Y faces
-  // centre sweep along X: A(r, q) at (x0-RC+r, y0-1-R+q)
-  for (int i = threadIdx.x; i < D::AYR * D::AYC; i += nt) {
-    const int r = i / D::AYC, q = i - r * D::AYC;
-    const int wr = r + (H - RC) - RC, wq = q + (H - 1 - R);
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      Tc acc = Tc(0);
-#pragma unroll
-      for (int k = 0; k < KC; ++k) acc = acc + c.w[k] * Ws[(v * D::WX + wr + k) * D::WY + wq];
-      A[(v * D::AYR + r) * D::AYC + q] = acc;
-    }
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < D::BYR * D::BYC; i += nt) {
-    const int r = i / D::BYC, f = i - r * D::BYC;
-    Tc wl[5], wr[5];
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      wl[v] = Tc(0);
-      wr[v] = Tc(0);
-    }
-#pragma unroll
-    for (int k = 0; k < KF; ++k) {
-      const int qa = f + k, qb = f + 1 + k;
+  // ---- Y faces: face f (y = y0+f) between cells y0+f-1 and y0+f; AY column
+  // of cell y is y - (y0-1-R). FW consecutive faces per thread.
+  {
+    constexpr int NGF = (TY + 1 + FW - 1) / FW;
+    constexpr int NWF = (KF + 2 * FW - 1) / FW;  // vectors covering columns f .. f+FW+KF-1
+    static_assert(4 * D::AYR * D::AYS + (D::AYR - 1) * D::AYS + (NGF - 1 + NWF) * FW <= D::S2,
+                  "Y-face reads past their shared region");
+    for (int i = threadIdx.x; i < D::BYR * NGF; i += nt) {
+      const int r = i / NGF, f = (i - r * NGF) * FW;
+      Tc wl[FW][5], wr[FW][5];
 #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        wl[v] = wl[v] + rrule.w[k] * A[(v * D::AYR + r) * D::AYC + qa];
-        wr[v] = wr[v] + lrule.w[k] * A[(v * D::AYR + r) * D::AYC + qb];
+        Tc x[NWF * FW];
+#pragma unroll
+        for (int n = 0; n < NWF; ++n) ldn<FW>(AY + (v * D::AYR + r) * D::AYS + f + n * FW, x + n * FW);
+#pragma unroll
+        for (int j = 0; j < FW; ++j) wl[j][v] = wr[j][v] = Tc(0);
+#pragma unroll
+        for (int k = 0; k < KF; ++k)
+#pragma unroll
+          for (int j = 0; j < FW; ++j) {
+            wl[j][v] = wl[j][v] + rrule.w[k] * x[j + k];
+            wr[j][v] = wr[j][v] + lrule.w[k] * x[j + 1 + k];
+          }
+      }
+#pragma unroll
+      for (int j = 0; j < FW; ++j) {
+        Tc fl[5];
+        riemann_flux<5>(ph, 5, wl[j], wr[j], g.dy, fl);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) BY[(v * D::BYR + r) * D::BYS + f + j] = fl[v];
       }
     }
-    Tc fl[5];
-    riemann_flux<5>(ph, 5, wl, wr, g.dy, fl);
-#pragma unroll
-    for (int v = 0; v < 5; ++v) B[(v * D::BYR + r) * D::BYC + f] = fl[v];
   }
   __syncthreads();
-  // transverse sweep along X -> GY TX x (TY+1)
-  for (int i = threadIdx.x; i < TX * (TY + 1); i += nt) {
-    const int r = i / (TY + 1), f = i - r * (TY + 1);
-    const int x = x0 + r, y = y0 + f;
-    Tc val[5];
+  // Y face fluxes: transverse sweep along X -> GY and G (owned faces)
+  sweep4<Tc, KC, 1, 0, TX, D::GYS / 4, D::BYS, D::BYR * D::BYS, D::S0>(
+      BY, t.w, [&](int v, int r, int f, const Tc* acc) {
+        stn<4>(GY + (v * TX + r) * D::GYS + f, acc);
+        const int x = x0 + r;
+        if (x < g.nx) {
+          Tc* o = G.p + G.at(x, y0 + f) + v * G.vs;
 #pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      Tc acc = Tc(0);
-#pragma unroll
-      for (int k = 0; k < KC; ++k) acc = acc + t.w[k] * B[(v * D::BYR + r + k) * D::BYC + f];
-      val[v] = acc;
-      GY[(v * TX + r) * (TY + 1) + f] = acc;
-    }
-    const bool owned = (f < TY || y == g.ny) && y <= g.ny && x < g.nx;
-    if (owned) {
-      Tc* o = G.p + G.at(x, y);
-#pragma unroll
-      for (int v = 0; v < 5; ++v) o[v * G.vs] = val[v];
-    }
-  }
+          for (int j = 0; j < 4; ++j) {
+            // faces y0..y0+TY-1, and y0+TY when it is the last face of the grid;
+            // columns past TY are padding
+            const int fj = f + j, y = y0 + fj;
+            if (fj <= TY && y <= g.ny && (fj < TY || y == g.ny)) o[j] = acc[j];
+          }
+        }
+      });
   if (!ustar) return;
   __syncthreads();
-  // candidate u* = u + dt (0 + cx (F[i+1]-F[i]) + cy (G[j+1]-G[j]))
-  const int plane = g.nx * g.ny;
-  for (int i = threadIdx.x; i < TX * TY; i += nt) {
-    const int r = i / TY, q = i - r * TY;
-    const int x = x0 + r, y = y0 + q;
-    if (x >= g.nx || y >= g.ny) continue;
-    const int o = x * g.ny + y;
+  // candidate u* = u + dt (0 + cx (F[i+1]-F[i]) + cy (G[j+1]-G[j])), four cells per thread
+  {
+    const int plane = g.nx * g.ny;
+    for (int i = threadIdx.x; i < TX * (TY / 4); i += nt) {
+      const int r = i / (TY / 4), q = (i - r * (TY / 4)) * 4;
+      const int x = x0 + r;
+      if (x >= g.nx) continue;
+      const int o = x * g.ny + y0 + q;
 #pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      Tc d = Tc(0);
-      d = d + (Tc)cx * (FX[(v * (TX + 1) + r + 1) * TY + q] - FX[(v * (TX + 1) + r) * TY + q]);
-      d = d + (Tc)cy * (GY[(v * TX + r) * (TY + 1) + q + 1] - GY[(v * TX + r) * (TY + 1) + q]);
-      ustar[v * plane + o] = (Tc)(u[v * plane + o] + dt * (double)d);
+      for (int v = 0; v < 5; ++v) {
+        Tc a[4], b[4], e[8];
+        ldn<4>(FX + (v * (TX + 1) + r) * TY + q, a);
+        ldn<4>(FX + (v * (TX + 1) + r + 1) * TY + q, b);
+        ldn<4>(GY + (v * TX + r) * D::GYS + q, e);
+        ldn<4>(GY + (v * TX + r) * D::GYS + q + 4, e + 4);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          if (y0 + q + j >= g.ny) continue;
+          Tc d = Tc(0);
+          d = d + (Tc)cx * (b[j] - a[j]);
+          d = d + (Tc)cy * (e[j + 1] - e[j]);
+          ustar[v * plane + o + j] = (Tc)(u[v * plane + o + j] + dt * (double)d);
+        }
+      }
     }
   }
   // predicted cells: their faces take the fallback flux now, blended as the
   // final pass would (the candidate above keeps the high-order fluxes)
   if (!pred || !tile_any<TX, TY>(pred, nullptr, g, x0, y0)) return;
   constexpr int PWX = TX + 4, PWY = TY + 4;
-  static_assert(PWX * PWY * 5 <= D::SW, "pointwise tile must fit in the W tile");
+  static_assert(PWX * PWY * 5 <= D::S0, "pointwise tile must fit in region 0");
   Tc* Pw = Ws;
   pointwise_tile<Tc, TX, TY>(u, g, x0, y0, Pw, ph);
   __syncthreads();
@@ -541,7 +671,7 @@ __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __res
     fallback_face_flux<Tc>(Pw + (r + 2) * PWY + f, PWX * PWY, 1, muscl, limiter, ph, g.dy, flo);
     Tc* o = G.p + G.at(x, y);
 #pragma unroll
-    for (int v = 0; v < 5; ++v) o[v * G.vs] = (Tc(1) - Tc(1)) * GY[(v * TX + r) * (TY + 1) + f] + Tc(1) * flo[v];
+    for (int v = 0; v < 5; ++v) o[v * G.vs] = (Tc(1) - Tc(1)) * GY[(v * TX + r) * D::GYS + f] + Tc(1) * flo[v];
   }
 }
 
