@@ -198,47 +198,55 @@ __device__ __forceinline__ void stn(double* p, const double* o) {
   }
 }
 
-// One stencil sweep over the five variable planes of a shared tile, four
+// Elements per shared-memory vector: one 16-byte access (4 floats, 2 doubles).
+template <typename Tc>
+struct VecW {
+  static constexpr int value = 16 / (int)sizeof(Tc);
+};
+
+// One stencil sweep over the five variable planes of a shared tile, VW
 // consecutive outputs of a row per thread:
-//   out(v, r, q) = sum_k w[k] in(v, r + k AR, OFF + q + k (1 - AR)),  r < NR, q < 4 NG,
+//   out(v, r, q) = sum_k w[k] in(v, r + k AR, OFF + q + k (1 - AR)),  r < NR, q < VW NG,
 // each sum accumulated from k = 0 upwards as a one-output loop accumulates it,
 // so every output is rounded exactly as before. AR = 1 puts the taps along the
-// strided axis (one aligned vector, or two when OFF is not a multiple of 4, per
-// tap), AR = 0 along the contiguous axis (one window of vectors per output
-// group). Row strides IS/OS and variable strides IVS/OVS are multiples of 4;
-// outputs past the caller's column count land in the padding of the output
-// rows. IN_LIM / OUT_LIM bound the elements the sweep may touch from `in` /
-// `out`. epi(v, r, q, acc) stores the four sums.
-template <typename Tc, int K, int AR, int OFF, int NR, int NG, int IS, int IVS, int IN_LIM, typename Epi>
-__device__ __forceinline__ void sweep4(const Tc* __restrict__ in, const Tc* __restrict__ w, Epi epi) {
-  constexpr int S = OFF & 3, B0 = OFF - S;
-  constexpr int NW = AR ? (S + 7) / 4 : (S + K + 6) / 4;
-  static_assert(IS % 4 == 0 && IVS % 4 == 0, "rows and planes must hold whole vectors");
-  static_assert(4 * IVS + (NR - 1 + (AR ? K - 1 : 0)) * IS + B0 + 4 * (NG - 1) + 4 * NW <= IN_LIM,
+// strided axis (one aligned vector, or two when OFF is not a multiple of VW,
+// per tap), AR = 0 along the contiguous axis (one window of vectors per output
+// group). Row strides IS and variable strides IVS are multiples of VW; outputs
+// past the caller's column count land in the padding of the output rows.
+// IN_LIM bounds the elements the sweep may read from `in`. epi(v, r, q, acc)
+// stores the VW sums.
+template <typename Tc, int VW, int K, int AR, int OFF, int NR, int NG, int IS, int IVS, int IN_LIM, typename Epi>
+__device__ __forceinline__ void sweepv(const Tc* __restrict__ in, const Tc* __restrict__ w, Epi epi) {
+  constexpr int S = OFF % VW, B0 = OFF - S;
+  constexpr int NW = AR ? (S + 2 * VW - 1) / VW : (S + K + 2 * VW - 2) / VW;
+  static_assert(IS % VW == 0 && IVS % VW == 0, "rows and planes must hold whole vectors");
+  static_assert(4 * IVS + (NR - 1 + (AR ? K - 1 : 0)) * IS + B0 + VW * (NG - 1) + VW * NW <= IN_LIM,
                 "sweep reads past its shared region");
   for (int i = threadIdx.x; i < NR * NG; i += blockDim.x) {
-    const int r = i / NG, q = (i - r * NG) * 4;
+    const int r = i / NG, q = (i - r * NG) * VW;
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
       const Tc* src = in + v * IVS + r * IS + B0 + q;
-      Tc acc[4] = {Tc(0), Tc(0), Tc(0), Tc(0)};
+      Tc acc[VW];
+#pragma unroll
+      for (int j = 0; j < VW; ++j) acc[j] = Tc(0);
       if constexpr (AR) {
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-          Tc x[4 * NW];
+          Tc x[VW * NW];
 #pragma unroll
-          for (int n = 0; n < NW; ++n) ldn<4>(src + k * IS + 4 * n, x + 4 * n);
+          for (int n = 0; n < NW; ++n) ldn<VW>(src + k * IS + VW * n, x + VW * n);
 #pragma unroll
-          for (int j = 0; j < 4; ++j) acc[j] = acc[j] + w[k] * x[S + j];
+          for (int j = 0; j < VW; ++j) acc[j] = acc[j] + w[k] * x[S + j];
         }
       } else {
-        Tc x[4 * NW];
+        Tc x[VW * NW];
 #pragma unroll
-        for (int n = 0; n < NW; ++n) ldn<4>(src + 4 * n, x + 4 * n);
+        for (int n = 0; n < NW; ++n) ldn<VW>(src + VW * n, x + VW * n);
 #pragma unroll
         for (int k = 0; k < K; ++k)
 #pragma unroll
-          for (int j = 0; j < 4; ++j) acc[j] = acc[j] + w[k] * x[S + j + k];
+          for (int j = 0; j < VW; ++j) acc[j] = acc[j] + w[k] * x[S + j + k];
       }
       epi(v, r, q, acc);
     }
@@ -461,14 +469,14 @@ struct FluxDims {
 #define FVH_FLUX_FW 2
 #endif
 // FW: faces per thread in the Riemann phases (1, 2 or 4)
-template <typename Tc, int P, int TX, int TY, int KC, int KF, int FW = FVH_FLUX_FW>
+template <typename Tc, int P, int TX, int TY, int KC, int KF, int FW = (sizeof(Tc) == 4 ? FVH_FLUX_FW : 1)>
 __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __restrict__ u, Geo g, V2<Tc> F, V2<Tc> G,
                                              Tc* __restrict__ ustar, Rule<Tc, KC> c, Rule<Tc, KC> t,
                                              Rule<Tc, KF> lrule, Rule<Tc, KF> rrule, Phys<Tc> ph, double cx,
                                              double cy, double dt, const uint8_t* __restrict__ pred, int muscl,
                                              int limiter, int bx, int by, unsigned char* smem_raw) {
   using D = FluxDims<P, TX, TY>;
-  constexpr int R = D::R, RC = D::RC, H = D::H, HY = D::HY;
+  constexpr int R = D::R, RC = D::RC, H = D::H, HY = D::HY, VW = VecW<Tc>::value;
   Tc* const S0 = reinterpret_cast<Tc*>(smem_raw);
   Tc* const S1 = S0 + D::S0;
   Tc* const S2 = S1 + D::S1;
@@ -482,40 +490,40 @@ __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __res
   const int nt = blockDim.x;
   const int x0 = by * TX, y0 = bx * TY;
   // W tile (W holds gW >= H ghosts; points that no output needs are clamped
-  // into range), four columns per access where W's rows are 16-byte aligned
+  // into range), VW columns per access where W's rows are 16-byte aligned
   {
-    constexpr int NG = D::WYS / 4;
-    const bool vec = ((W.g | W.sx | W.vs) & 3) == 0 && (reinterpret_cast<uintptr_t>(W.p) & 15) == 0;
+    constexpr int NG = D::WYS / VW;
+    const bool vec = ((W.g | W.sx | W.vs) & (VW - 1)) == 0 && (reinterpret_cast<uintptr_t>(W.p) & 15) == 0;
     for (int i = threadIdx.x; i < D::WX * NG; i += nt) {
-      const int r = i / NG, cq = (i - r * NG) * 4;
+      const int r = i / NG, cq = (i - r * NG) * VW;
       const int x = min(max(x0 - H + r, -W.g), g.nx + W.g - 1), y = y0 - HY + cq;
-      Tc val[5][4];
-      if (vec && y >= -W.g && y + 3 <= g.ny + W.g - 1) {
+      Tc val[5][VW];
+      if (vec && y >= -W.g && y + VW - 1 <= g.ny + W.g - 1) {
         const Tc* p = W.p + W.at(x, y);
 #pragma unroll
-        for (int v = 0; v < 5; ++v) ldn<4>(p + v * W.vs, val[v]);
+        for (int v = 0; v < 5; ++v) ldn<VW>(p + v * W.vs, val[v]);
       } else {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < VW; ++j) {
           const Tc* p = W.p + W.at(x, min(max(y + j, -W.g), g.ny + W.g - 1));
 #pragma unroll
           for (int v = 0; v < 5; ++v) val[v][j] = p[v * W.vs];
         }
       }
 #pragma unroll
-      for (int v = 0; v < 5; ++v) stn<4>(Ws + (v * D::WX + r) * D::WYS + cq, val[v]);
+      for (int v = 0; v < 5; ++v) stn<VW>(Ws + (v * D::WX + r) * D::WYS + cq, val[v]);
     }
   }
   __syncthreads();
   // centre sweeps of both directions from the W tile
   // X faces: AX(r, q) at (x0-1-R+r, y0-RC+q), taps along Y
-  sweep4<Tc, KC, 0, HY - 2 * RC, D::AXR, D::AXS / 4, D::WYS, D::WX * D::WYS, D::S0 - (H - 1 - R) * D::WYS>(
+  sweepv<Tc, VW, KC, 0, HY - 2 * RC, D::AXR, D::AXS / VW, D::WYS, D::WX * D::WYS, D::S0 - (H - 1 - R) * D::WYS>(
       Ws + (H - 1 - R) * D::WYS, c.w,
-      [&](int v, int r, int q, const Tc* acc) { stn<4>(AX + (v * D::AXR + r) * D::AXS + q, acc); });
+      [&](int v, int r, int q, const Tc* acc) { stn<VW>(AX + (v * D::AXR + r) * D::AXS + q, acc); });
   // Y faces: AY(r, q) at (x0-RC+r, y0-1-R+q), taps along X
-  sweep4<Tc, KC, 1, HY - 1 - R, D::AYR, D::AYS / 4, D::WYS, D::WX * D::WYS, D::S0 - (H - 2 * RC) * D::WYS>(
+  sweepv<Tc, VW, KC, 1, HY - 1 - R, D::AYR, D::AYS / VW, D::WYS, D::WX * D::WYS, D::S0 - (H - 2 * RC) * D::WYS>(
       Ws + (H - 2 * RC) * D::WYS, c.w,
-      [&](int v, int r, int q, const Tc* acc) { stn<4>(AY + (v * D::AYR + r) * D::AYS + q, acc); });
+      [&](int v, int r, int q, const Tc* acc) { stn<VW>(AY + (v * D::AYR + r) * D::AYS + q, acc); });
   __syncthreads();
   // ---- X faces: face f (x = x0+f) between cells x0+f-1 and x0+f; AX row of
   // cell x is x - (x0-1-R). FW consecutive columns per thread.
@@ -550,14 +558,14 @@ __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __res
   }
   __syncthreads();
   // X face fluxes: transverse sweep along Y -> FX and F (owned faces)
-  sweep4<Tc, KC, 0, 0, D::BXR, TY / 4, D::AXS, D::BXR * D::AXS, D::S0>(
+  sweepv<Tc, VW, KC, 0, 0, D::BXR, TY / VW, D::AXS, D::BXR * D::AXS, D::S0>(
       BX, t.w, [&](int v, int f, int q, const Tc* acc) {
-        stn<4>(FX + (v * (TX + 1) + f) * TY + q, acc);
+        stn<VW>(FX + (v * (TX + 1) + f) * TY + q, acc);
         const int x = x0 + f;
         if ((f < TX || x == g.nx) && x <= g.nx) {
           Tc* o = F.p + F.at(x, y0 + q) + v * F.vs;
 #pragma unroll
-          for (int j = 0; j < 4; ++j)
+          for (int j = 0; j < VW; ++j)
             if (y0 + q + j < g.ny) o[j] = acc[j];
         }
       });
@@ -598,14 +606,14 @@ __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __res
   }
   __syncthreads();
   // Y face fluxes: transverse sweep along X -> GY and G (owned faces)
-  sweep4<Tc, KC, 1, 0, TX, D::GYS / 4, D::BYS, D::BYR * D::BYS, D::S0>(
+  sweepv<Tc, VW, KC, 1, 0, TX, D::GYS / VW, D::BYS, D::BYR * D::BYS, D::S0>(
       BY, t.w, [&](int v, int r, int f, const Tc* acc) {
-        stn<4>(GY + (v * TX + r) * D::GYS + f, acc);
+        stn<VW>(GY + (v * TX + r) * D::GYS + f, acc);
         const int x = x0 + r;
         if (x < g.nx) {
           Tc* o = G.p + G.at(x, y0 + f) + v * G.vs;
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
+          for (int j = 0; j < VW; ++j) {
             // faces y0..y0+TY-1, and y0+TY when it is the last face of the grid;
             // columns past TY are padding
             const int fj = f + j, y = y0 + fj;
@@ -615,23 +623,23 @@ __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __res
       });
   if (!ustar) return;
   __syncthreads();
-  // candidate u* = u + dt (0 + cx (F[i+1]-F[i]) + cy (G[j+1]-G[j])), four cells per thread
+  // candidate u* = u + dt (0 + cx (F[i+1]-F[i]) + cy (G[j+1]-G[j])), VW cells per thread
   {
     const int plane = g.nx * g.ny;
-    for (int i = threadIdx.x; i < TX * (TY / 4); i += nt) {
-      const int r = i / (TY / 4), q = (i - r * (TY / 4)) * 4;
+    for (int i = threadIdx.x; i < TX * (TY / VW); i += nt) {
+      const int r = i / (TY / VW), q = (i - r * (TY / VW)) * VW;
       const int x = x0 + r;
       if (x >= g.nx) continue;
       const int o = x * g.ny + y0 + q;
 #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        Tc a[4], b[4], e[8];
-        ldn<4>(FX + (v * (TX + 1) + r) * TY + q, a);
-        ldn<4>(FX + (v * (TX + 1) + r + 1) * TY + q, b);
-        ldn<4>(GY + (v * TX + r) * D::GYS + q, e);
-        ldn<4>(GY + (v * TX + r) * D::GYS + q + 4, e + 4);
+        Tc a[VW], b[VW], e[2 * VW];
+        ldn<VW>(FX + (v * (TX + 1) + r) * TY + q, a);
+        ldn<VW>(FX + (v * (TX + 1) + r + 1) * TY + q, b);
+        ldn<VW>(GY + (v * TX + r) * D::GYS + q, e);
+        ldn<VW>(GY + (v * TX + r) * D::GYS + q + VW, e + VW);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < VW; ++j) {
           if (y0 + q + j >= g.ny) continue;
           Tc d = Tc(0);
           d = d + (Tc)cx * (b[j] - a[j]);
@@ -684,7 +692,7 @@ struct DtSpec {
 };
 
 template <typename Tc, int P, int TX, int TY, int KC, int KF>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(Tc) == 4 ? 4 : 3)
     k2_fluxes(V2<const Tc> W, const double* __restrict__ u, Geo g, V2<Tc> F, V2<Tc> G, Tc* __restrict__ ustar,
               Rule<Tc, KC> c, Rule<Tc, KC> t, Rule<Tc, KF> lrule, Rule<Tc, KF> rrule, Phys<Tc> ph, double cx,
               double cy, Scalars* __restrict__ sc, DtSpec dts, const uint8_t* __restrict__ pred, int muscl,
@@ -830,6 +838,118 @@ __global__ void __launch_bounds__(256)
 // primitives of the stage input with 2 ghosts), the blend with the
 // high-order fluxes, the divergence and the Runge-Kutta combination.
 // ---------------------------------------------------------------------------
+// The Runge-Kutta combination of one cell's five variables at o + v*plane
+// (fvhoe/ode.py:245-298; the expressions of k_final, evaluated in the same
+// order) for integrator INTEG at stage STAGE. Every array the stage reads is
+// loaded for all five variables before the first store, so a cell's loads are
+// in flight together. Returns how many results are not finite.
+template <int INTEG, int STAGE>
+__device__ __forceinline__ unsigned int rk_combine(const StageSpec& st, int o, int plane, double dt,
+                                                   const double* k) {
+  double a[5], b[5], res[5];
+  if constexpr (INTEG == INT_RHS) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      st.dudt_out[o + v * plane] = k[v];
+      res[v] = k[v];
+    }
+  } else if constexpr (INTEG == INT_EULER) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) a[v] = st.u[o + v * plane];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      res[v] = a[v] + dt * k[v];
+      st.u[o + v * plane] = res[v];
+    }
+  } else if constexpr (INTEG == INT_SSPRK2) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      a[v] = st.u[o + v * plane];
+      if constexpr (STAGE != 0) b[v] = st.stage_in[o + v * plane];
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      if constexpr (STAGE == 0) {
+        res[v] = a[v] + dt * k[v];
+        st.next[o + v * plane] = res[v];
+      } else {
+        res[v] = 0.5 * a[v] + 0.5 * (b[v] + dt * k[v]);
+        st.u[o + v * plane] = res[v];
+      }
+    }
+  } else if constexpr (INTEG == INT_SSPRK3) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      a[v] = st.u[o + v * plane];
+      if constexpr (STAGE != 0) b[v] = st.acc[o + v * plane];
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const int ov = o + v * plane;
+      if constexpr (STAGE == 0) {
+        st.acc[ov] = k[v];
+        res[v] = a[v] + dt * k[v];
+        st.next[ov] = res[v];
+      } else if constexpr (STAGE == 1) {
+        const double qd = 0.25 * dt;
+        res[v] = (a[v] + qd * b[v]) + qd * k[v];
+        st.next[ov] = res[v];
+        st.acc[ov] = b[v] + k[v];
+      } else {
+        res[v] = a[v] + ((1.0 / 6.0) * dt) * (b[v] + 4.0 * k[v]);
+        st.u[ov] = res[v];
+      }
+    }
+  } else {  // INT_RK4
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      a[v] = st.u[o + v * plane];
+      if constexpr (STAGE != 0) b[v] = st.acc[o + v * plane];
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const int ov = o + v * plane;
+      if constexpr (STAGE == 0) {
+        st.acc[ov] = k[v];
+        res[v] = a[v] + (0.5 * dt) * k[v];
+        st.next[ov] = res[v];
+      } else if constexpr (STAGE == 1 || STAGE == 2) {
+        st.acc[ov] = b[v] + 2.0 * k[v];
+        res[v] = a[v] + (STAGE == 1 ? 0.5 * dt : dt) * k[v];
+        st.next[ov] = res[v];
+      } else {
+        res[v] = a[v] + ((1.0 / 6.0) * dt) * (b[v] + k[v]);
+        st.u[ov] = res[v];
+      }
+    }
+  }
+  unsigned int bad = 0;
+#pragma unroll
+  for (int v = 0; v < 5; ++v) bad += isfinite(res[v]) ? 0u : 1u;
+  return bad;
+}
+
+// rk_combine for the integrator and stage named at run time (the batched ensemble)
+__device__ __forceinline__ unsigned int rk_combine_rt(const StageSpec& st, int o, int plane, double dt,
+                                                      const double* k) {
+  switch (st.integrator) {
+    case INT_RHS: return rk_combine<INT_RHS, 0>(st, o, plane, dt, k);
+    case INT_EULER: return rk_combine<INT_EULER, 0>(st, o, plane, dt, k);
+    case INT_SSPRK2:
+      return st.stage == 0 ? rk_combine<INT_SSPRK2, 0>(st, o, plane, dt, k)
+                           : rk_combine<INT_SSPRK2, 1>(st, o, plane, dt, k);
+    case INT_SSPRK3:
+      if (st.stage == 0) return rk_combine<INT_SSPRK3, 0>(st, o, plane, dt, k);
+      if (st.stage == 1) return rk_combine<INT_SSPRK3, 1>(st, o, plane, dt, k);
+      return rk_combine<INT_SSPRK3, 2>(st, o, plane, dt, k);
+    default:
+      if (st.stage == 0) return rk_combine<INT_RK4, 0>(st, o, plane, dt, k);
+      if (st.stage == 1) return rk_combine<INT_RK4, 1>(st, o, plane, dt, k);
+      if (st.stage == 2) return rk_combine<INT_RK4, 2>(st, o, plane, dt, k);
+      return rk_combine<INT_RK4, 3>(st, o, plane, dt, k);
+  }
+}
+
 template <int TX, int TY>
 struct FinalDims {
   static constexpr int PX = TX + 4, PY = TY + 4;
@@ -838,7 +958,8 @@ struct FinalDims {
   static constexpr int SG = TX * (TY + 1) * 5;
 };
 
-template <typename Tc, int TX, int TY>
+// RKI < 0: the integrator and stage are read from st at run time.
+template <typename Tc, int TX, int TY, int RKI = -1, int RKS = 0>
 __device__ __forceinline__ void tile2_final(const double* __restrict__ stage_in, Geo g, V2<const Tc> F,
                                             V2<const Tc> G, const uint8_t* __restrict__ trouble,
                                             const uint8_t* __restrict__ pred, int apost, int muscl, int limiter,
@@ -908,89 +1029,62 @@ __device__ __forceinline__ void tile2_final(const double* __restrict__ stage_in,
   }
   __syncthreads();
   // divergence and the Runge-Kutta combination
-  const double dt = st.integrator == INT_RHS ? 0.0 : dt_step;
+  const double dt = (RKI >= 0 ? RKI : st.integrator) == INT_RHS ? 0.0 : dt_step;
   const int plane = g.nx * g.ny;
   unsigned int bad = 0;
   for (int i = threadIdx.x; i < TX * TY; i += nt) {
     const int r = i / TY, q = i - r * TY;
     const int x = x0 + r, y = y0 + q;
     if (x >= g.nx || y >= g.ny) continue;
-    const int base = x * g.ny + y;
+    double k[5];
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
       Tc dc = Tc(0);
       dc = dc + (Tc)cx * (FX[(v * (TX + 1) + r + 1) * TY + q] - FX[(v * (TX + 1) + r) * TY + q]);
       dc = dc + (Tc)cy * (GY[(v * TX + r) * (TY + 1) + q + 1] - GY[(v * TX + r) * (TY + 1) + q]);
-      const int o = base + v * plane;
-      const double k = (double)dc;
-      double res = 0.0;
-      switch (st.integrator) {
-        case INT_RHS:
-          st.dudt_out[o] = k;
-          res = k;
-          break;
-        case INT_EULER:
-          res = st.u[o] + dt * k;
-          st.u[o] = res;
-          break;
-        case INT_SSPRK2:
-          if (st.stage == 0) {
-            res = st.u[o] + dt * k;
-            st.next[o] = res;
-          } else {
-            res = 0.5 * st.u[o] + 0.5 * (st.stage_in[o] + dt * k);
-            st.u[o] = res;
-          }
-          break;
-        case INT_SSPRK3:
-          if (st.stage == 0) {
-            st.acc[o] = k;
-            res = st.u[o] + dt * k;
-            st.next[o] = res;
-          } else if (st.stage == 1) {
-            const double a = st.acc[o];
-            const double qd = 0.25 * dt;
-            res = (st.u[o] + qd * a) + qd * k;
-            st.next[o] = res;
-            st.acc[o] = a + k;
-          } else {
-            res = st.u[o] + ((1.0 / 6.0) * dt) * (st.acc[o] + 4.0 * k);
-            st.u[o] = res;
-          }
-          break;
-        case INT_RK4:
-          if (st.stage == 0) {
-            st.acc[o] = k;
-            res = st.u[o] + (0.5 * dt) * k;
-            st.next[o] = res;
-          } else if (st.stage == 1) {
-            st.acc[o] = st.acc[o] + 2.0 * k;
-            res = st.u[o] + (0.5 * dt) * k;
-            st.next[o] = res;
-          } else if (st.stage == 2) {
-            st.acc[o] = st.acc[o] + 2.0 * k;
-            res = st.u[o] + dt * k;
-            st.next[o] = res;
-          } else {
-            res = st.u[o] + ((1.0 / 6.0) * dt) * (st.acc[o] + k);
-            st.u[o] = res;
-          }
-          break;
-      }
-      bad += isfinite(res) ? 0u : 1u;
+      k[v] = (double)dc;
+    }
+    if constexpr (RKI >= 0) {
+      bad += rk_combine<RKI, RKS>(st, x * g.ny + y, plane, dt, k);
+    } else {
+      bad += rk_combine_rt(st, x * g.ny + y, plane, dt, k);
     }
   }
   block_count_add(bad, &sc->nonfinite);
 }
 
-template <typename Tc, int TX, int TY>
-__global__ void __launch_bounds__(256)
+// RKI / RKS: the integrator and stage of the launch (one instantiation each)
+template <typename Tc, int TX, int TY, int RKI, int RKS>
+__global__ void __launch_bounds__(256, sizeof(Tc) == 4 ? 5 : 3)
     k2_final(const double* __restrict__ stage_in, Geo g, V2<const Tc> F, V2<const Tc> G,
              const uint8_t* __restrict__ trouble, const uint8_t* __restrict__ pred, int apost, int muscl, int limiter,
              Phys<Tc> ph, double cx, double cy, StageSpec st, Scalars* __restrict__ sc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  tile2_final<Tc, TX, TY>(stage_in, g, F, G, trouble, pred, apost, muscl, limiter, ph, cx, cy, st,
-                          st.integrator == INT_RHS ? 0.0 : sc->dt_step, sc, blockIdx.x, blockIdx.y, smem_raw);
+  tile2_final<Tc, TX, TY, RKI, RKS>(stage_in, g, F, G, trouble, pred, apost, muscl, limiter, ph, cx, cy, st,
+                                    RKI == INT_RHS ? 0.0 : sc->dt_step, sc, blockIdx.x, blockIdx.y, smem_raw);
+}
+
+template <typename Tc, int TX, int TY>
+using FinalKernel = void (*)(const double*, Geo, V2<const Tc>, V2<const Tc>, const uint8_t*, const uint8_t*, int,
+                             int, int, Phys<Tc>, double, double, StageSpec, Scalars*);
+
+// The k2_final instantiation of an integrator and stage.
+template <typename Tc, int TX, int TY>
+FinalKernel<Tc, TX, TY> final_kernel(int integrator, int stage) {
+  switch (integrator) {
+    case INT_EULER: return k2_final<Tc, TX, TY, INT_EULER, 0>;
+    case INT_SSPRK2: return stage == 0 ? k2_final<Tc, TX, TY, INT_SSPRK2, 0> : k2_final<Tc, TX, TY, INT_SSPRK2, 1>;
+    case INT_SSPRK3:
+      if (stage == 0) return k2_final<Tc, TX, TY, INT_SSPRK3, 0>;
+      if (stage == 1) return k2_final<Tc, TX, TY, INT_SSPRK3, 1>;
+      return k2_final<Tc, TX, TY, INT_SSPRK3, 2>;
+    case INT_RK4:
+      if (stage == 0) return k2_final<Tc, TX, TY, INT_RK4, 0>;
+      if (stage == 1) return k2_final<Tc, TX, TY, INT_RK4, 1>;
+      if (stage == 2) return k2_final<Tc, TX, TY, INT_RK4, 2>;
+      return k2_final<Tc, TX, TY, INT_RK4, 3>;
+    default: return k2_final<Tc, TX, TY, INT_RHS, 0>;
+  }
 }
 
 }  // namespace f2

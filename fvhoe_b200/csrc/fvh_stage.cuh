@@ -683,7 +683,7 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
   {
     using D = f2::FinalDims<T::EX, T::EY>;
     const size_t smem = (size_t)(D::SP + D::SF + D::SG) * sizeof(Tc);
-    auto kern = f2::k2_final<Tc, T::EX, T::EY>;
+    auto kern = f2::final_kernel<Tc, T::EX, T::EY>(c.spec.integrator, c.spec.stage);
     set_smem((const void*)kern, smem);
     const dim3 grid((g.ny + T::EY - 1) / T::EY, (g.nx + T::EX - 1) / T::EX);
     int arrays = 1;
