@@ -135,9 +135,9 @@ constexpr int kPrimTX = 16, kPrimTY = 32;
 template <typename Tc, int P, int TX, int TY>
 struct Smem {
   static constexpr int R = (P + 1) / 2, RC = P / 2;
-  using DP = f2::PrimsDims<P, kPrimTX, kPrimTY>;
+  using DP = f2::PrimsDims<Tc, P, kPrimTX, kPrimTY>;
   using DF = f2::FluxDims<P, TX, TY>;
-  using DD = f2::PrimsDims<P, TX + 6, TY + 6>;
+  using DD = f2::PrimsDims<Tc, P, TX + 6, TY + 6>;
   using DE = f2::FinalDims<TX, TY>;
   static constexpr int prim = (DP::A + DP::B) * (int)sizeof(Tc);
   static constexpr int flux = DF::TOTAL * (int)sizeof(Tc);

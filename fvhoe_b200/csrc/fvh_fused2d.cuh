@@ -254,86 +254,89 @@ __device__ __forceinline__ void sweepv(const Tc* __restrict__ in, const Tc* __re
 }
 
 // Tile dimensions of the primitive computation producing OX x OY outputs
-// with degree P (centre / transverse rules of radius RC = P / 2).
-template <int P, int OX, int OY>
+// with degree P (centre / transverse rules of radius RC = P / 2) in the
+// compute type Tc. Rows are padded to whole 16-byte vectors (LYS, PYS, OYS);
+// PAD is slack after each buffer for the reads that feed padding outputs.
+template <typename Tc, int P, int OX, int OY>
 struct PrimsDims {
+  static constexpr int VW = VecW<Tc>::value;
   static constexpr int RC = P / 2;
   static constexpr int LX = OX + 4 * RC, LY = OY + 4 * RC;  // loaded state
   static constexpr int CX = OX + 2 * RC;                    // after the X centre sweep: CX x LY
   static constexpr int PY = OY + 2 * RC;                    // after the Y centre sweep: CX x PY
+  static constexpr int LYS = (LY + VW - 1) / VW * VW, PYS = (PY + VW - 1) / VW * VW, OYS = (OY + VW - 1) / VW * VW;
+  static constexpr int PAD = 16;
   // after the X transverse sweep: OX x PY; after the Y transverse sweep: OX x OY (in A)
-  static constexpr int A = Max<Max<LX * LY, CX * PY>::value, OX * OY>::value * 5;
-  static constexpr int B = Max<CX * LY, OX * PY>::value * 5;
+  static constexpr int A = Max<Max<LX * LYS, CX * PYS>::value, OX * OYS>::value * 5 + PAD;
+  static constexpr int B = Max<CX * LYS, OX * PYS>::value * 5 + PAD;
 };
 
 // W on [x0, x0+OX) x [y0, y0+OY), computed in two shared buffers; the result
-// is left in A as an OX x OY tile. Rules: centre c and transverse t (KC taps).
+// is left in A as an OX x OY tile with row stride OYS. Rules: centre c and
+// transverse t (KC taps). The sweeps run VW outputs per thread (sweepv), each
+// output summed in the order of a one-output loop.
 template <typename Tc, int P, int OX, int OY, int KC, typename Tin>
 __device__ __forceinline__ void primitives_tile(const Tin* __restrict__ u, const Geo& g, int x0, int y0, Tc* A,
                                                 Tc* B, const Rule<Tc, KC>& c, const Rule<Tc, KC>& t,
                                                 const Phys<Tc>& ph) {
-  using D = PrimsDims<P, OX, OY>;
-  constexpr int RC = D::RC;
+  using D = PrimsDims<Tc, P, OX, OY>;
+  constexpr int RC = D::RC, VW = VecW<Tc>::value;
   const int nt = blockDim.x;
-  // 1. state with 2*RC ghosts around the tile
+  // 1. state with 2*RC ghosts around the tile: A, LX x LYS
   for (int i = threadIdx.x; i < D::LX * D::LY; i += nt) {
     const int r = i / D::LY, q = i - r * D::LY;
     Tc s[5];
     load_state2<Tc>(u, g, x0 - 2 * RC + r, y0 - 2 * RC + q, s);
 #pragma unroll
-    for (int v = 0; v < 5; ++v) A[(v * D::LX + r) * D::LY + q] = s[v];
+    for (int v = 0; v < 5; ++v) A[(v * D::LX + r) * D::LYS + q] = s[v];
   }
   __syncthreads();
-  // 2. centre sweep along X
-  for (int i = threadIdx.x; i < D::CX * D::LY; i += nt) {
-    const int r = i / D::LY, q = i - r * D::LY;
+  // 2. centre sweep along X: B, CX x LYS
+  sweepv<Tc, VW, KC, 1, 0, D::CX, D::LYS / VW, D::LYS, D::LX * D::LYS, D::A>(
+      A, c.w, [&](int v, int r, int q, const Tc* acc) { stn<VW>(B + (v * D::CX + r) * D::LYS + q, acc); });
+  __syncthreads();
+  // 3. centre sweep along Y, then primitives: A, CX x PYS
+  {
+    constexpr int NG = D::PYS / VW, NW = (KC + 2 * VW - 2) / VW;
+    static_assert(4 * D::CX * D::LYS + (D::CX - 1) * D::LYS + VW * (NG - 1 + NW) <= D::B,
+                  "centre sweep reads past its shared region");
+    for (int i = threadIdx.x; i < D::CX * NG; i += nt) {
+      const int r = i / NG, q = (i - r * NG) * VW;
+      Tc acc[5][VW];
 #pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      Tc acc = Tc(0);
+      for (int v = 0; v < 5; ++v) {
+        Tc x[VW * NW];
 #pragma unroll
-      for (int k = 0; k < KC; ++k) acc = acc + c.w[k] * A[(v * D::LX + r + k) * D::LY + q];
-      B[(v * D::CX + r) * D::LY + q] = acc;
+        for (int n = 0; n < NW; ++n) ldn<VW>(B + (v * D::CX + r) * D::LYS + q + VW * n, x + VW * n);
+#pragma unroll
+        for (int j = 0; j < VW; ++j) {
+          acc[v][j] = Tc(0);
+#pragma unroll
+          for (int k = 0; k < KC; ++k) acc[v][j] = acc[v][j] + c.w[k] * x[j + k];
+        }
+      }
+      Tc w[5][VW];
+#pragma unroll
+      for (int j = 0; j < VW; ++j) {
+        Tc a5[5], w5[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) a5[v] = acc[v][j];
+        to_primitives(ph, 5, a5, w5);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) w[v][j] = w5[v];
+      }
+#pragma unroll
+      for (int v = 0; v < 5; ++v) stn<VW>(A + (v * D::CX + r) * D::PYS + q, w[v]);
     }
   }
   __syncthreads();
-  // 3. centre sweep along Y, then primitives
-  for (int i = threadIdx.x; i < D::CX * D::PY; i += nt) {
-    const int r = i / D::PY, q = i - r * D::PY;
-    Tc acc[5], w[5];
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      acc[v] = Tc(0);
-#pragma unroll
-      for (int k = 0; k < KC; ++k) acc[v] = acc[v] + c.w[k] * B[(v * D::CX + r) * D::LY + q + k];
-    }
-    to_primitives(ph, 5, acc, w);
-#pragma unroll
-    for (int v = 0; v < 5; ++v) A[(v * D::CX + r) * D::PY + q] = w[v];
-  }
+  // 4. transverse sweep along X: B, OX x PYS
+  sweepv<Tc, VW, KC, 1, 0, OX, D::PYS / VW, D::PYS, D::CX * D::PYS, D::A>(
+      A, t.w, [&](int v, int r, int q, const Tc* acc) { stn<VW>(B + (v * OX + r) * D::PYS + q, acc); });
   __syncthreads();
-  // 4. transverse sweep along X
-  for (int i = threadIdx.x; i < OX * D::PY; i += nt) {
-    const int r = i / D::PY, q = i - r * D::PY;
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      Tc acc = Tc(0);
-#pragma unroll
-      for (int k = 0; k < KC; ++k) acc = acc + t.w[k] * A[(v * D::CX + r + k) * D::PY + q];
-      B[(v * OX + r) * D::PY + q] = acc;
-    }
-  }
-  __syncthreads();
-  // 5. transverse sweep along Y, into A as an OX x OY tile
-  for (int i = threadIdx.x; i < OX * OY; i += nt) {
-    const int r = i / OY, q = i - r * OY;
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      Tc acc = Tc(0);
-#pragma unroll
-      for (int k = 0; k < KC; ++k) acc = acc + t.w[k] * B[(v * OX + r) * D::PY + q + k];
-      A[(v * OX + r) * OY + q] = acc;
-    }
-  }
+  // 5. transverse sweep along Y, into A as an OX x OYS tile
+  sweepv<Tc, VW, KC, 0, 0, OX, D::OYS / VW, D::PYS, OX * D::PYS, D::B>(
+      B, t.w, [&](int v, int r, int q, const Tc* acc) { stn<VW>(A + (v * OX + r) * D::OYS + q, acc); });
   __syncthreads();
 }
 
@@ -382,7 +385,7 @@ template <typename Tc, int P, int TX, int TY, int KC, bool REDUCE>
 __device__ __forceinline__ void tile2_primitives(const double* __restrict__ u, Geo g, V2<Tc> W, int gw_out,
                                                  Rule<Tc, KC> c, Rule<Tc, KC> t, Phys<Tc> ph, ReduceSpec rs,
                                                  Scalars* __restrict__ sc, int bx, int by, unsigned char* smem_raw) {
-  using D = PrimsDims<P, TX, TY>;
+  using D = PrimsDims<Tc, P, TX, TY>;
   Tc* A = reinterpret_cast<Tc*>(smem_raw);
   Tc* B = A + D::A;
   const int x0 = -gw_out + by * TX;
@@ -400,7 +403,7 @@ __device__ __forceinline__ void tile2_primitives(const double* __restrict__ u, G
     if (x >= g.nx + gw_out || y >= g.ny + gw_out) continue;
     Tc w[5];
 #pragma unroll
-    for (int v = 0; v < 5; ++v) w[v] = A[(v * TX + r) * TY + q];
+    for (int v = 0; v < 5; ++v) w[v] = A[(v * TX + r) * D::OYS + q];
     Tc* o = W.p + W.at(x, y);
 #pragma unroll
     for (int v = 0; v < 5; ++v) o[v * W.vs] = w[v];
@@ -723,7 +726,7 @@ __device__ __forceinline__ void tile2_detect(const Tc* __restrict__ ustar, Geo g
                                              double* __restrict__ log_nad, double* __restrict__ log_pad, int bx,
                                              int by, unsigned char* smem_raw) {
   constexpr int OX = TX + 6, OY = TY + 6;
-  using D = PrimsDims<P, OX, OY>;
+  using D = PrimsDims<Tc, P, OX, OY>;
   Tc* A = reinterpret_cast<Tc*>(smem_raw);
   Tc* B = A + D::A;
   const int x0 = by * TX, y0 = bx * TY;
@@ -772,7 +775,7 @@ __device__ __forceinline__ void tile2_detect(const Tc* __restrict__ ustar, Geo g
           big = fmax(big, xv);
           small = fmin(small, xv);
         }
-      const Tc* ps = A + (v * OX + r + 3) * OY + q + 3;
+      const Tc* ps = A + (v * OX + r + 3) * D::OYS + q + 3;
       const Tc xs = ps[0];
       Tc ind;
       bool tv;
@@ -790,7 +793,7 @@ __device__ __forceinline__ void tile2_detect(const Tc* __restrict__ ustar, Geo g
       if (tv && ds.sed) {
         Tc line[7];
 #pragma unroll
-        for (int m = 0; m < 7; ++m) line[m] = ps[(m - 3) * OY];
+        for (int m = 0; m < 7; ++m) line[m] = ps[(m - 3) * D::OYS];
         bool below = sed_line_below_one(line, sed_eps);
         if (!below) {
 #pragma unroll

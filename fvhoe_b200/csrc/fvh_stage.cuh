@@ -603,7 +603,7 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
   }
   // 1. W with gW ghosts + reductions
   {
-    using D = f2::PrimsDims<P, T::PX, T::PY>;
+    using D = f2::PrimsDims<Tc, P, T::PX, T::PY>;
     const size_t smem = (size_t)(D::A + D::B) * sizeof(Tc);
     auto kern = f2::k2_primitives<Tc, P, T::PX, T::PY, KC, true>;
     set_smem((const void*)kern, smem);
@@ -666,7 +666,7 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     ds.force_trouble = cfg.force_trouble;
     ds.log_mode = cfg.log_troubles ? c.log_mode : 0;
     ds.log_div = ds.log_mode ? c.log_div : 0.0;
-    using D = f2::PrimsDims<P, T::DX + 6, T::DY + 6>;
+    using D = f2::PrimsDims<Tc, P, T::DX + 6, T::DY + 6>;
     const size_t smem = (size_t)(D::A + D::B) * sizeof(Tc);
     auto kern = f2::k2_detect<Tc, P, T::DX, T::DY, KC>;
     set_smem((const void*)kern, smem);
