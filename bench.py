@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--pred-snapshots", type=int, default=16, help="stages sampled per training run")
     ap.add_argument("--pred-epochs", type=int, default=2)
     ap.add_argument("--pred-accuracy-time", type=float, default=0.002)
+    ap.add_argument("--pred-every", type=int, default=3,
+                    help="stages between predictions of the second learned form (3: once per SSP-RK3 step)")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
     ap.add_argument("--ens-members", type=int, default=256)
     ap.add_argument("--ens-steps", type=int, default=10, help="timed ensemble steps")
@@ -349,22 +351,26 @@ def predictor_leg(args, stream, sp):
     n, p = args.pred_n, args.pred_p
     cells = n * n
 
-    def make(precision, with_pred):
+    def make(precision, every=0):
         s = EulerSolver(precision=precision, **solver_kwargs(n, p, seed=0))
-        if with_pred:
-            s.set_predictor(net, threshold=0.5)
+        if every:
+            s.set_predictor(net, threshold=0.5, every=every)
         return s
 
-    plain = make("fp64", False)
-    fused = make("fp32", False)
-    learned = make("fp32", True)
+    k = args.pred_every
+    plain = make("fp64")
+    fused = make("fp32")
+    learned = make("fp32", every=1)
+    learned_k = make("fp32", every=k)
     t_acc = args.pred_accuracy_time
-    for s in (plain, fused, learned):
+    for s in (plain, fused, learned, learned_k):
         s.ssprk3(t_acc)
     rho = plain.am("u")[0]
     l1_fused = float(torch.mean(torch.abs(fused.am("u")[0] - rho)).item())
     l1_learned = float(torch.mean(torch.abs(learned.am("u")[0] - rho)).item())
+    l1_learned_k = float(torch.mean(torch.abs(learned_k.am("u")[0] - rho)).item())
     rates = learned.predictor_rates()
+    rates_k = learned_k.predictor_rates()
 
     def timed(s):
         h = s._handle
@@ -376,6 +382,8 @@ def predictor_leg(args, stream, sp):
     v_plain, ms_plain = timed(plain)
     v_fused, ms_fused = timed(fused)
     v_learned, ms_learned = timed(learned)
+    v_learned_k, ms_learned_k = timed(learned_k)
+    lk = f"fp32_fused_learned_every{k}"
     # kernel shares of the predictor form
     h = learned._handle
     _capi.check(lib.fvh_profile_enable(h, 1), h)
@@ -396,12 +404,18 @@ def predictor_leg(args, stream, sp):
                      "source": f"plain FP64 solver, KH seeds 101/102 and a four-quadrant run at {nt}^2, "
                                f"p={args.pred_p}, one stage every {every} steps over {steps} steps",
                      "held_out": held_rates},
-        "mcell_updates_per_s": {"plain_fp64": v_plain, "fp32_fused": v_fused, "fp32_fused_learned": v_learned},
-        "ms_per_step": {"plain_fp64": ms_plain, "fp32_fused": ms_fused, "fp32_fused_learned": ms_learned},
-        "speedup_vs_plain_fp64": {"fp32_fused": v_fused / v_plain, "fp32_fused_learned": v_learned / v_plain},
+        "prediction_interval": {"fp32_fused_learned": "every stage",
+                                lk: f"every {k} stages, flags reused in between"},
+        "mcell_updates_per_s": {"plain_fp64": v_plain, "fp32_fused": v_fused, "fp32_fused_learned": v_learned,
+                                lk: v_learned_k},
+        "ms_per_step": {"plain_fp64": ms_plain, "fp32_fused": ms_fused, "fp32_fused_learned": ms_learned,
+                        lk: ms_learned_k},
+        "speedup_vs_plain_fp64": {"fp32_fused": v_fused / v_plain, "fp32_fused_learned": v_learned / v_plain,
+                                  lk: v_learned_k / v_plain},
         "l1_density_error_vs_fp64": {"t": t_acc, "steps": plain.step_count, "fp32_fused": l1_fused,
-                                     "fp32_fused_learned": l1_learned},
+                                     "fp32_fused_learned": l1_learned, lk: l1_learned_k},
         "rates_over_l1_run": rates,
+        "rates_over_l1_run_every": {lk: rates_k},
         "kernel_shares_learned": shares,
         "tensor_core_wait_errors": errors,
     }

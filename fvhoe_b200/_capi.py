@@ -59,6 +59,7 @@ EXPORTS = (
     "fvh_mlp_logits",
     "fvh_mlp_errors",
     "fvh_set_predictor",
+    "fvh_set_predictor_interval",
     "fvh_get_pred_stats",
     "fvh_pred_flags",
     "fvh_boundary_layout",
@@ -198,6 +199,7 @@ def _load():
     lib.fvh_mlp_errors.argtypes = [vp]
     lib.fvh_mlp_errors.restype = ctypes.c_uint
     lib.fvh_set_predictor.argtypes = [vp, vp, ctypes.c_float]
+    lib.fvh_set_predictor_interval.argtypes = [vp, ctypes.c_int]
     lib.fvh_get_pred_stats.argtypes = [vp, ctypes.POINTER(FvhPredStats), vp]
     lib.fvh_pred_flags.argtypes = [vp, vp, vp]
     ip = ctypes.POINTER(ctypes.c_int)
@@ -232,7 +234,7 @@ def _load():
                  "fvh_trouble_log", "fvh_set_log_mode", "fvh_get_stats", "fvh_profile_enable", "fvh_profile_read",
                  "fvh_mlp_create", "fvh_mlp_destroy", "fvh_mlp_get_params", "fvh_mlp_set_params", "fvh_mlp_features",
                  "fvh_mlp_train_step", "fvh_mlp_gradients", "fvh_mlp_logits", "fvh_set_predictor",
-                 "fvh_get_pred_stats", "fvh_pred_flags"):
+                 "fvh_set_predictor_interval", "fvh_get_pred_stats", "fvh_pred_flags"):
         getattr(lib, name).restype = ctypes.c_int
     return lib
 

@@ -48,8 +48,10 @@ struct fvh_handle {
 
   // learned troubled-cell predictor (optional)
   fvh_mlp* mlp = nullptr;         // attached network (not owned)
-  uint8_t* pred = nullptr;        // predicted flags of the last stage
+  uint8_t* pred = nullptr;        // predicted flags of the last prediction
   float pred_thr_logit = 0.0f;    // logit threshold
+  int pred_interval = 1;          // stages between predictions (flags reused in between)
+  long long pred_stage = 0;       // fused stages run since the predictor was attached
   bool last_stage_fused = false;  // the last stage ran the fused 2D kernels
 
   int log_mode_next = 1;          // log mode of the next stage

@@ -737,6 +737,18 @@ int fvh_set_predictor(fvh_handle* h, fvh_mlp* m, float threshold) {
   }
   h->mlp = m;
   h->pred_thr_logit = std::log(threshold / (1.0f - threshold));
+  h->pred_stage = 0;
+  return FVH_OK;
+}
+
+int fvh_set_predictor_interval(fvh_handle* h, int stages) {
+  if (!h) return FVH_ERR_ARG;
+  if (stages < 1) {
+    h->err = "the prediction interval is a positive number of stages";
+    return FVH_ERR_ARG;
+  }
+  h->pred_interval = stages;
+  h->pred_stage = 0;
   return FVH_OK;
 }
 

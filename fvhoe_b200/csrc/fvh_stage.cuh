@@ -629,10 +629,12 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
   dts.use_fixed = cfg.use_fixed_dt;
   dts.first_stage = c.first_stage;
   dts.has_target = c.has_target;
-  // learned predictor: flags from W and the extrema just reduced
+  // learned predictor: flags from W and the extrema just reduced, refreshed
+  // every pred_interval stages and reused in between
   const uint8_t* pred = nullptr;
   if (h->mlp && apost) {
-    if ((st = mlp_predict_stage(h, s))) return st;
+    if (h->pred_stage % h->pred_interval == 0 && (st = mlp_predict_stage(h, s))) return st;
+    ++h->pred_stage;
     pred = h->pred;
   }
   const f2::V2<Tc> F = f2::make_v2((Tc*)h->F[ax[0]], g.nx + 1, g.ny, 0);

@@ -352,13 +352,17 @@ class EulerSolver(ODE):
                     self._handle)
 
     # -- learned troubled-cell predictor (no counterpart in the reference) ------
-    def set_predictor(self, predictor, threshold: float = 0.5):
+    def set_predictor(self, predictor, threshold: float = 0.5, every: int = 1):
         """Attaches a TroubledCellPredictor (None detaches). Needs the fused 2D
         path, a-posteriori limiting and global NAD. Faces next to predicted
         cells take the fallback flux; the a-posteriori check still runs on every
-        cell and revises the faces of cells the network missed."""
+        cell and revises the faces of cells the network missed. The network runs
+        every `every` stages and its flags are reused in the stages between."""
         m = predictor._m if predictor is not None else None
+        if int(every) < 1:
+            raise ValueError("every must be a positive number of stages")
         self._capi.check(self._capi.lib.fvh_set_predictor(self._handle, m, float(threshold)), self._handle)
+        self._capi.check(self._capi.lib.fvh_set_predictor_interval(self._handle, int(every)), self._handle)
         self._predictor = predictor
         self.pred_totals = dict(predicted=0, troubled=0, missed=0, false_alarm=0, cell_stages=0)
 

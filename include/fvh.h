@@ -302,6 +302,13 @@ unsigned int fvh_mlp_errors(fvh_mlp* m);
  * global NAD and a network on h's device; m must outlive the attachment. */
 int fvh_set_predictor(fvh_handle* h, fvh_mlp* m, float threshold);
 
+/* Runs the attached predictor every `stages` fused stages (default 1, every
+ * stage) and reuses its flags in the stages between; the a-posteriori check
+ * still judges every cell of every stage and revises the misses. Attaching a
+ * predictor restarts the count. No counterpart in the reference (its detector
+ * has no predictor). */
+int fvh_set_predictor_interval(fvh_handle* h, int stages);
+
 /* Predictor counts of the last step, summed over its stages. */
 typedef struct fvh_pred_stats {
   unsigned int predicted;   /* cells the network flagged */

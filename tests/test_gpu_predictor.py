@@ -190,3 +190,31 @@ def test_trained_predictor_gains_over_untrained():
     print("attached", r)
     assert r["missed"] < 0.2 * r["troubled"]
     assert net.errors() == 0
+
+
+@pytest.mark.parametrize("every,launches", [(1, 6), (2, 3), (3, 2)])
+def test_prediction_interval(every, launches):
+    """With an interval of k stages the network runs on stages 0, k, 2k, ... and
+    the stages between reuse its flags; the a-posteriori check still judges
+    every stage, so the predictor counts cover all of them."""
+    import ctypes
+
+    from fvhoe_b200 import _capi
+
+    n = 64
+    s = _kh_solver(n, 1)
+    s.set_predictor(_net(3), threshold=0.5, every=every)
+    lib, h = _capi.lib, s._handle
+    _capi.check(lib.fvh_profile_enable(h, 1), h)
+    s.ssprk3(n=2)
+    K = len(_capi.KERNEL_KINDS)
+    ms = (ctypes.c_double * K)()
+    count = (ctypes.c_uint64 * K)()
+    _capi.check(lib.fvh_profile_read(h, ms, None, count, s._stream()), h)
+    _capi.check(lib.fvh_profile_enable(h, 0), h)
+    assert count[_capi.KERNEL_KINDS.index("predict")] == launches
+    r = s.predictor_rates()
+    assert r["cell_stages"] == 6 * n * n
+    assert 0 <= r["missed"] <= r["troubled"]
+    with pytest.raises(ValueError):
+        s.set_predictor(_net(3), every=0)
