@@ -154,10 +154,13 @@ __global__ void __launch_bounds__(128, 4)
   __shared__ uint64_t bar;
   __shared__ uint32_t tmem_slot;
   copy_bytes(B1, img, kImgB1 + kImgB2);
+  // the hidden layers carry doubled activations (gelu2): the second layer's
+  // accumulator is halved in its bias FMA and w3 is stored halved, so every
+  // value equals the plain forward pass bit for bit
   for (int i = threadIdx.x; i < kHidden; i += blockDim.x) {
     pb[i] = params[kB1 + i];
     pb[64 + i] = params[kB2 + i];
-    pb[128 + i] = params[kW3 + i];
+    pb[128 + i] = 0.5f * params[kW3 + i];
   }
   if (threadIdx.x == 0) pb[192] = params[kB3];
   block_tmem_setup(&tmem_slot, &bar);
@@ -195,7 +198,7 @@ __global__ void __launch_bounds__(128, 4)
       float h[16];
       tc::tmem_ld16(tb + lane + (uint32_t)(16 * c), h);
 #pragma unroll
-      for (int j = 0; j < 16; ++j) h[j] = gelu(h[j] + pb[16 * c + j]);
+      for (int j = 0; j < 16; ++j) h[j] = gelu2(h[j] + pb[16 * c + j]);
       *reinterpret_cast<uint4*>(A2 + tc::kmajor_offset(r, 16 * c, kRows)) = pack_bf16x8(h);
       *reinterpret_cast<uint4*>(A2 + tc::kmajor_offset(r, 16 * c + 8, kRows)) = pack_bf16x8(h + 8);
     }
@@ -206,7 +209,8 @@ __global__ void __launch_bounds__(128, 4)
       float h[16];
       tc::tmem_ld16(tb + lane + (uint32_t)(64 + 16 * c), h);
 #pragma unroll
-      for (int j = 0; j < 16; ++j) logit = fmaf(gelu(h[j] + pb[64 + 16 * c + j]), pb[128 + 16 * c + j], logit);
+      for (int j = 0; j < 16; ++j)
+        logit = fmaf(gelu2(fmaf(h[j], 0.5f, pb[64 + 16 * c + j])), pb[128 + 16 * c + j], logit);
     }
     if (valid) pred[cell] = logit > thr_logit ? 1 : 0;
     tc::fence_before_sync();

@@ -59,6 +59,12 @@ __device__ __forceinline__ float gelu(float x) {
   const float t = tanh_approx(kGeluC * fmaf(kGeluA * x, x * x, x));
   return 0.5f * x * (1.0f + t);
 }
+// 2 gelu(x), rounded exactly as gelu(x) and doubled (the inference kernel keeps
+// doubled activations: a power-of-two scale that BF16 and FP32 carry exactly)
+__device__ __forceinline__ float gelu2(float x) {
+  const float t = tanh_approx(kGeluC * fmaf(kGeluA * x, x * x, x));
+  return x * (1.0f + t);
+}
 __device__ __forceinline__ float gelu_grad(float x) {
   const float t = tanh_approx(kGeluC * fmaf(kGeluA * x, x * x, x));
   return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * kGeluC * fmaf(3.0f * kGeluA, x * x, 1.0f);
@@ -90,7 +96,7 @@ __device__ __forceinline__ uint4 pack_bf16x8(const float* v) {
 template <typename Tw, int C>
 __device__ __forceinline__ uint4 feature_chunk(const Tw* __restrict__ W, int sx, int vs, int o, const int* vid,
                                                const float* inv_s) {
-  constexpr float kNorm = 0.08685882093641431f;  // 1 / ln(1 + 1e5)
+  constexpr float kNorm2 = 0.060205946838836726f;  // ln 2 / ln(1 + 1e5): log2 scaled to the normalised log
   float f[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
@@ -102,7 +108,7 @@ __device__ __forceinline__ uint4 feature_chunk(const Tw* __restrict__ W, int sx,
     const int v = k / 25, a = (k % 25) / 5 - 2, b = (k % 5) - 2;
     const Tw* base = W + vid[v] * vs + o;
     const float d = (float)(base[a * sx + b] - base[0]);
-    const float m = __logf(fmaf(fabsf(d), inv_s[v], 1.0f)) * kNorm;
+    const float m = __log2f(fmaf(fabsf(d), inv_s[v], 1.0f)) * kNorm2;
     f[i] = d < 0.0f ? -m : m;
   }
   return pack_bf16x8(f);
