@@ -25,13 +25,66 @@ def _hit_target(t: float, dt: float, target: float = None) -> float:
     return dt
 
 
+class SnapshotList(list):
+    """The snapshot list (a plain list of dicts in the reference). Snapshots may
+    be copied to the host asynchronously; every read of the list first calls
+    settle(), which waits for the copies still in flight and completes their
+    entries, so a reader always sees finished arrays. It pickles as a plain list."""
+
+    def __init__(self, settle, items=()):
+        super().__init__(items)
+        self._settle = settle
+
+    def __getitem__(self, i):
+        self._settle()
+        return super().__getitem__(i)
+
+    def __iter__(self):
+        self._settle()
+        return super().__iter__()
+
+    def __reversed__(self):
+        self._settle()
+        return super().__reversed__()
+
+    def __contains__(self, x):
+        self._settle()
+        return super().__contains__(x)
+
+    def __eq__(self, other):
+        self._settle()
+        return list.__eq__(self, other)
+
+    __hash__ = None
+
+    def __repr__(self):
+        self._settle()
+        return super().__repr__()
+
+    def copy(self):
+        self._settle()
+        return list(super().__iter__())
+
+    def index(self, *args):
+        self._settle()
+        return super().index(*args)
+
+    def count(self, x):
+        self._settle()
+        return super().count(x)
+
+    def __reduce_ex__(self, protocol):
+        self._settle()
+        return (list, (list(super().__iter__()),))
+
+
 class ODE(ABC):
     def _ode_init(self, progress_bar: bool = True):
         self.t = 0.0
         self.timestamps = [0.0]
         self.step_count = 0
         self.timer = Timer(cats=["TOTAL", "SNAPSHOTS"])
-        self.snapshots = []
+        self.snapshots = SnapshotList(self._settle_snapshots)
         self.snapshot_times = []
         self.print_progress_bar = bool(progress_bar)
         self.integrator = None
@@ -58,6 +111,9 @@ class ODE(ABC):
     def snapshot(self):
         self.snapshots.append(None)
         self.snapshot_times.append(self.t)
+
+    def _settle_snapshots(self):
+        """Completes snapshots whose host copies are still in flight (none here)."""
 
     def read_snapshots(self) -> bool:
         return False

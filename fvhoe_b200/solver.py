@@ -28,7 +28,7 @@ from .boundary_conditions import BoundaryCondition
 from .fv import fv_average, fv_uniform_meshgen
 from .hydro import HydroState, compute_conservatives
 from .initial_conditions import InitialCondition, Square
-from .ode import ODE
+from .ode import ODE, SnapshotList
 
 _VAR_INDEX = {"rho": 0, "vx": 1, "mx": 1, "vy": 2, "my": 2, "vz": 3, "mz": 3, "P": 4, "E": 4}
 _STAGES = {"euler": 1, "ssprk2": 2, "ssprk3": 3, "rk4": 4}
@@ -399,11 +399,10 @@ class EulerSolver(ODE):
         return out.cpu().numpy()
 
     def _init_array_allocation(self):
-        import torch
-
         self.am.add("w", np.zeros((self.nvars,) + self.n))
         self._dudt = None
-        self._log_tmp = torch.empty((3,) + self.n, dtype=torch.float64, device=self.am("u").device)
+        self._copy_stream = None  # snapshot copies to the host
+        self._pending_snapshots = []
 
     def __del__(self):
         handle = getattr(self, "_handle", None)
@@ -524,38 +523,91 @@ class EulerSolver(ODE):
         )
         return w
 
-    def _trouble_logs(self):
-        t = self._log_tmp
+    def _trouble_logs_device(self):
+        """The trouble logs of the run so far (trouble count, NAD and PAD
+        magnitudes) as a new (3,) + n device tensor."""
+        import torch
+
+        t = torch.empty((3,) + self.n, dtype=torch.float64, device=self.am("u").device)
         self._capi.check(
             self._capi.lib.fvh_trouble_log(self._handle, 0.0, ctypes.c_void_p(t[0].data_ptr()),
                                            ctypes.c_void_p(t[1].data_ptr()), ctypes.c_void_p(t[2].data_ptr()),
                                            self._stream()),
             self._handle,
         )
-        host = t.cpu().numpy()
+        return t
+
+    def _trouble_logs(self):
+        """The trouble logs as three (5,) + n host arrays (synchronous)."""
+        host = self._trouble_logs_device().cpu().numpy()
         return [np.broadcast_to(host[i], (5,) + self.n).copy() for i in range(3)]
+
+    def _host_copy(self, t):
+        """Enqueues the copy of device tensor t into pinned host memory on the
+        snapshot copy stream, after the work queued so far on the solver's
+        stream, and returns the host tensor (complete once the copy is)."""
+        import torch
+
+        main = torch.cuda.current_stream(t.device)
+        if self._copy_stream is None:
+            self._copy_stream = torch.cuda.Stream(device=t.device)
+        cs = self._copy_stream
+        cs.wait_stream(main)
+        h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+        with torch.cuda.stream(cs):
+            h.copy_(t, non_blocking=True)
+        t.record_stream(cs)
+        return h
 
     # -- snapshots (fvhoe/solver.py:835-953) -----------------------------------------
     def snapshot(self):
-        self.am("w").copy_(self.primitives(fv_average=self.snapshots_as_fv_averages))
-        log = {"x": self.x, "y": self.y, "z": self.z, "t": self.t, "w": self.am.get_numpy("w")}
-        if self.a_posteriori_slope_limiting:
-            if self._log_enabled:
-                trouble, nad, pad = self._trouble_logs()
-            else:
-                trouble = nad = pad = np.zeros((5,) + self.n)
-            log["trouble"] = trouble
-            log["NAD violation magnitude"] = nad
-            log["PAD violation magnitude"] = pad
+        """Records the snapshot dict of the reference (x, y, z, t, w and, with
+        limiting, the trouble logs). The primitives and logs are computed on the
+        device and copied to pinned host memory on a separate stream, so the
+        copies overlap the following steps; reading `snapshots` (or calling the
+        snapshot helper) first waits for the copies still in flight."""
+        w = self.primitives(fv_average=self.snapshots_as_fv_averages)
+        self.am("w").copy_(w)
+        log = {"x": self.x, "y": self.y, "z": self.z, "t": self.t, "w": None}
+        host_w = self._host_copy(w)
+        apost = self.a_posteriori_slope_limiting
+        host_logs = self._host_copy(self._trouble_logs_device()) if apost and self._log_enabled else None
+        event = self._copy_stream.record_event()
+        n = self.n
+
+        def finish():
+            log["w"] = host_w.numpy()
+            if apost:
+                if host_logs is not None:
+                    host = host_logs.numpy()
+                    trouble, nad, pad = [np.broadcast_to(host[i], (5,) + n).copy() for i in range(3)]
+                else:
+                    trouble = nad = pad = np.zeros((5,) + n)
+                log["trouble"] = trouble
+                log["NAD violation magnitude"] = nad
+                log["PAD violation magnitude"] = pad
+
+        self._pending_snapshots.append((event, finish))
         self.snapshots.append(log)
         self.snapshot_times.append(self.t)
         if self.snapshot_helper_function is not None:
+            self._settle_snapshots()
             self.snapshot_helper_function(self)
+
+    def _settle_snapshots(self):
+        """Waits for the snapshot copies in flight and completes their entries."""
+        pending = getattr(self, "_pending_snapshots", None)
+        if not pending:
+            return
+        self._pending_snapshots = []
+        for event, finish in pending:
+            event.synchronize()
+            finish()
 
     def read_snapshots(self) -> bool:
         if os.path.exists(self.snapshot_dir):
             with open(os.path.join(self.snapshot_dir, "arrs.pkl"), "rb") as fh:
-                self.snapshots = pickle.load(fh)
+                self.snapshots = SnapshotList(self._settle_snapshots, pickle.load(fh))
             print(f"Read from snapshot directory {self.snapshot_dir}")
             return True
         return False

@@ -233,3 +233,24 @@ def test_initial_conditions_match_oracle_setup():
     c, d = load(os.path.join(GOLDEN, "steps_sedov3d16_p3.npz"))
     X, Y, Z = fv_uniform_meshgen((16, 16, 16))
     assert np.array_equal(SedovBlast(dims="xyz").build_ic(hs)(X, Y, Z), d["u0"])
+
+
+def test_snapshot_list_settles_before_reads_and_pickles_as_a_list():
+    """Snapshots are completed lazily: every read of the list waits for the
+    copies in flight first (settle), taking the length does not, and the list
+    pickles as the reference's plain list."""
+    import pickle
+
+    from fvhoe_b200.ode import SnapshotList
+
+    calls = []
+    log = SnapshotList(lambda: calls.append(1))
+    log.append({"t": 0.0})
+    log.append({"t": 0.5})
+    assert len(log) == 2 and not calls
+    assert log[-1]["t"] == 0.5 and len(calls) == 1
+    assert [d["t"] for d in log] == [0.0, 0.5] and len(calls) == 2
+    assert log == [{"t": 0.0}, {"t": 0.5}]
+    back = pickle.loads(pickle.dumps(log))
+    assert type(back) is list and back == [{"t": 0.0}, {"t": 0.5}]
+    assert type(log.copy()) is list

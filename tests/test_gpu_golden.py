@@ -145,3 +145,37 @@ def test_log_division_in_the_last_stage_equals_the_separate_pass():
     for a, b in zip(*logs):
         assert np.array_equal(a, b)
     assert logs[0][0].max() > 0
+
+
+def test_snapshots_copied_asynchronously_equal_settled_ones(tmp_path):
+    """Snapshot copies run on a separate stream and are completed when the list
+    is read: a run that reads nothing until it ends records the same snapshots
+    (primitives and trouble logs) as one whose helper reads each snapshot as it
+    is taken, and the pickled snapshots read back unchanged."""
+    from fvhoe_b200 import EulerSolver, KelvinHelmholtzNoise2D
+
+    def make():
+        return EulerSolver(w0=KelvinHelmholtzNoise2D(n=(96, 64), seed=5), nx=96, ny=64, px=5, py=5, gamma=1.4,
+                           a_posteriori_slope_limiting=True, NAD=1e-5, progress_bar=False)
+
+    lazy = make()
+    lazy.ssprk3(0.02, downbeats=[0.005, 0.01, 0.015], log_every_step=False)
+    seen = []
+    eager = make()
+    eager.snapshot_helper_function = lambda s: seen.append(
+        (s.snapshots[-1]["w"].copy(), s.am.get_numpy("w"), s.snapshots[-1]["trouble"].copy()))
+    eager.ssprk3(0.02, downbeats=[0.005, 0.01, 0.015], log_every_step=False)
+    assert len(lazy.snapshots) == len(seen) == 5
+    for got, (w_eager, w_device, trouble) in zip(lazy.snapshots, seen):
+        assert np.array_equal(w_eager, w_device)
+        assert np.array_equal(got["w"], w_eager)
+        assert np.array_equal(got["trouble"], trouble)
+        assert list(got) == ["x", "y", "z", "t", "w", "trouble", "NAD violation magnitude",
+                             "PAD violation magnitude"]
+    assert lazy.snapshots[-1]["trouble"].max() > 0
+    lazy.snapshot_dir = str(tmp_path / "snaps")
+    lazy.write_snapshots(overwrite=False)
+    back = make()
+    back.snapshot_dir = lazy.snapshot_dir
+    assert back.read_snapshots()
+    assert all(np.array_equal(a["w"], b["w"]) for a, b in zip(lazy.snapshots, back.snapshots))
