@@ -81,10 +81,13 @@ def workload_config(args, n=None):
 
 
 def solver_kwargs(n, p, seed):
+    """The KH workload; its initial state is averaged on the device (every
+    solver of a comparison starts from the same state)."""
     from fvhoe_b200 import KelvinHelmholtzNoise2D
 
     return dict(w0=KelvinHelmholtzNoise2D(n=(n, n), seed=seed), nx=n, ny=n, px=p, py=p, gamma=1.4,
-                riemann_solver="hllc", CFL=0.8, a_posteriori_slope_limiting=True, NAD=1e-5, progress_bar=False)
+                riemann_solver="hllc", CFL=0.8, a_posteriori_slope_limiting=True, NAD=1e-5, progress_bar=False,
+                ic_on_device=True)
 
 
 # ---------------------------------------------------------------------------
@@ -330,7 +333,7 @@ def predictor_leg(args, stream, sp):
             EulerSolver(**solver_kwargs(nt, args.pred_p, seed=102)),
             EulerSolver(w0=FourQuadrant2D(seed=103), nx=nt, ny=nt, px=args.pred_p, py=args.pred_p, gamma=1.4,
                         riemann_solver="hllc", CFL=0.8, bc=BoundaryCondition(x="outflow", y="outflow"),
-                        a_posteriori_slope_limiting=True, NAD=1e-5, progress_bar=False)]
+                        a_posteriori_slope_limiting=True, NAD=1e-5, progress_bar=False, ic_on_device=True)]
     X, y = collect_training_data(runs, steps=steps, every=every)
     del runs
     torch.cuda.synchronize()

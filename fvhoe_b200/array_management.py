@@ -57,6 +57,19 @@ class ArrayManager:
             array = torch.from_numpy(np.ascontiguousarray(array)).to(self.device)
         self.arrays[name] = array
 
+    def add_device(self, name: str, tensor):
+        """Registers a float64 device tensor already on this manager's device
+        (no copy; "cuda" backend only)."""
+        if self.backend != "cuda":
+            raise TypeError("add_device needs the cuda backend")
+        if name in self.arrays:
+            raise KeyError(f"Array with name '{name}' already exists.")
+        import torch
+
+        if not isinstance(tensor, torch.Tensor) or tensor.device.type != "cuda" or tensor.dtype != torch.float64:
+            raise TypeError("add_device takes a float64 CUDA tensor")
+        self.arrays[name] = tensor.contiguous()
+
     def _check_name(self, name: str):
         if name not in self.arrays:
             raise KeyError(f"Array with name '{name}' not found.")

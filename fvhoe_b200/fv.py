@@ -1,9 +1,11 @@
-"""Mesh and finite-volume averaging of initial conditions (host, set-up only).
+"""Mesh and finite-volume averaging of initial conditions (set-up only).
 
 Same interfaces as fvhoe/fv.py:12-85 (`fv_uniform_meshgen`; the ghost-slab
 coordinates are `slab_meshgen`) and :227-277 (`fv_average` with
-Gauss-Legendre quadrature). These run on the host: the averaging once per
-solver, the slab coordinates once per solver with Dirichlet boundaries.
+Gauss-Legendre quadrature). These run once per solver: the averaging on the
+host, or on the device for the library's initial conditions with
+`EulerSolver(ic_on_device=True)`; the slab coordinates of Dirichlet
+boundaries on the host.
 """
 
 from functools import lru_cache
@@ -11,6 +13,8 @@ from itertools import product
 from typing import Callable, Dict, Tuple
 
 import numpy as np
+
+from .array_ns import of
 
 
 def fv_uniform_meshgen(n, x=(0, 1), y=(0, 1), z=(0, 1)):
@@ -63,12 +67,15 @@ def legendre_quadrature(p: int) -> Tuple[np.ndarray, np.ndarray]:
     return nodes / 2, weights / 2
 
 
-def fv_average(f: Callable, x, y, z, h, p=(0, 0, 0)) -> np.ndarray:
-    """Cell averages of f(x, y, z) by tensor-product Gauss-Legendre quadrature."""
+def fv_average(f: Callable, x, y, z, h, p=(0, 0, 0)):
+    """Cell averages of f(x, y, z) by tensor-product Gauss-Legendre quadrature,
+    for host arrays or device tensors (the same sums in the same order)."""
     rules = [legendre_quadrature(pi) for pi in p]
-    out = np.zeros_like(f(x, y, z))
-    for xp, xw in zip(*rules[0]):
-        for yp, yw in zip(*rules[1]):
-            for zp, zw in zip(*rules[2]):
-                out += (xw * yw * zw) * f(x=x + xp * h[0], y=y + yp * h[1], z=z + zp * h[2])
+    first = f(x, y, z)
+    out = of(first).zeros_like(first)
+    for xq, xw in zip(*rules[0]):
+        for yq, yw in zip(*rules[1]):
+            for zq, zw in zip(*rules[2]):
+                out += float(xw * yw * zw) * f(x=x + float(xq * h[0]), y=y + float(yq * h[1]),
+                                               z=z + float(zq * h[2]))
     return out

@@ -11,6 +11,8 @@ from typing import Tuple, Union
 
 import numpy as np
 
+from .array_ns import of
+
 
 class HydroState:
     def __init__(self, passive_scalars: tuple = (), ndim: int = 4):
@@ -81,15 +83,16 @@ class HydroState:
 
 
 def compute_conservatives(hs: HydroState, w: np.ndarray, gamma: float) -> np.ndarray:
-    """Host conversion used to build initial conditions (fvhoe/hydro.py:173-196)."""
-    u = np.empty_like(w)
+    """Conversion used to build initial conditions (fvhoe/hydro.py:173-196), for
+    host arrays or device tensors (array_ns)."""
+    u = of(w).empty_like(w)
     rho = w[0]
     u[0] = rho
     u[1:4] = rho * w[1:4]
     ke = u[1] * w[1]
     ke = ke + u[2] * w[2]
     ke = ke + u[3] * w[3]
-    u[4] = w[4] / (gamma - 1) + 0.5 * ke
+    u[4] = of(w).div(w[4], gamma - 1) + 0.5 * ke
     if w.shape[0] > 5:
         u[5:] = rho * w[5:]
     return u

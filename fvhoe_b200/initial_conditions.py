@@ -17,6 +17,8 @@ from typing import Callable, Dict, Sequence, Tuple
 
 import numpy as np
 
+from .array_ns import of
+
 
 class InitialCondition(ABC):
     def __init__(self, *args, **kwargs):
@@ -35,7 +37,7 @@ class InitialCondition(ABC):
         core = self.base_ic(*self.args, **self.kwargs)
 
         def ic_func(x, y, z):
-            out = np.empty((5 + len(hs.passive_scalars),) + np.shape(x))
+            out = of(x).empty((5 + len(hs.passive_scalars),) + tuple(np.shape(x)), like=x)
             out[:5] = core(x, y, z)
             for name in hs.passive_scalars:
                 out[hs.variable_map[name]] = passive_ic_funcs[name](x, y, z)
@@ -44,8 +46,9 @@ class InitialCondition(ABC):
         return ic_func
 
 
-def _state(shape, rho, vx, vy, vz, P):
-    out = np.empty((5,) + tuple(shape))
+def _state(like, rho, vx, vy, vz, P):
+    """(5,) + like.shape primitive state in like's namespace."""
+    out = of(like).empty((5,) + tuple(like.shape), like=like)
     out[0], out[1], out[2], out[3], out[4] = rho, vx, vy, vz, P
     return out
 
@@ -55,11 +58,12 @@ class Sinus(InitialCondition):
 
     def base_ic(self, dims="x", rho_min_max=(1, 2), P=1, vx=1, vy=0, vz=0):
         def f(x, y=None, z=None):
-            r = np.zeros_like(x)
+            xp = of(x)
+            r = xp.zeros_like(x)
             for d, c in zip("xyz", (x, y, z)):
                 r = r + (c if d in dims else 0)
             lo, span = rho_min_max[0], rho_min_max[1] - rho_min_max[0]
-            return _state(r.shape, span * (0.5 * np.sin(2 * np.pi * r) + 0.5) + lo, vx, vy, vz, P)
+            return _state(r, span * (0.5 * xp.sin(2 * xp.pi * r) + 0.5) + lo, vx, vy, vz, P)
 
         return f
 
@@ -69,11 +73,12 @@ class Square(InitialCondition):
 
     def base_ic(self, dims="x", rho_min_max=(1, 2), P=1, vx=1, vy=0, vz=0):
         def f(x, y=None, z=None):
-            inside = np.ones_like(x, dtype=bool)
+            xp = of(x)
+            inside = xp.mask_like(x)
             for d, c in zip("xyz", (x, y, z)):
                 if d in dims:
                     inside &= (c > 0.25) & (c < 0.75)
-            return _state(x.shape, np.where(inside, rho_min_max[1], rho_min_max[0]), vx, vy, vz, P)
+            return _state(x, xp.where(inside, rho_min_max[1], rho_min_max[0]), vx, vy, vz, P)
 
         return f
 
@@ -87,11 +92,12 @@ class Shock1D(InitialCondition):
             raise ValueError("dim must be 'x', 'y', or 'z'")
 
         def f(x, y=None, z=None):
+            xp = of(x)
             r = {"x": x, "y": y, "z": z}[dim]
             left = r < position
-            v = np.where(left, v_left_right[0], v_left_right[1])
+            v = xp.where(left, v_left_right[0], v_left_right[1])
             vel = [v if dim == d else 0 for d in "xyz"]
-            return _state(r.shape, np.where(left, *rho_left_right), *vel, np.where(left, *P_left_right))
+            return _state(r, xp.where(left, *rho_left_right), *vel, xp.where(left, *P_left_right))
 
         return f
 
@@ -101,13 +107,14 @@ class DoubleShock1D(InitialCondition):
 
     def base_ic(self, dim="x", positions=(0.1, 0.9), rhos=(1, 1, 1), vs=(0, 0, 0), Ps=(10**3, 10**-2, 10**2)):
         def f(x, y=None, z=None):
+            xp = of(x)
             r = {"x": x, "y": y, "z": z}[dim]
 
             def pick(vals):
-                return np.where(r < positions[0], vals[0], np.where(r < positions[1], vals[1], vals[2]))
+                return xp.where(r < positions[0], vals[0], xp.where(r < positions[1], vals[1], vals[2]))
 
             vel = [pick(vs) if dim == d else 0 for d in "xyz"]
-            return _state(r.shape, pick(rhos), *vel, pick(Ps))
+            return _state(r, pick(rhos), *vel, pick(Ps))
 
         return f
 
@@ -117,12 +124,13 @@ class ShuOsher1D(InitialCondition):
 
     def base_ic(self, dim="x"):
         def f(x, y=None, z=None):
+            xp = of(x)
             r = {"x": x, "y": y, "z": z}[dim] - 5
             post = r < -4
-            v = np.where(post, 2.629369, 0)
+            v = xp.where(post, 2.629369, 0)
             vel = [v if dim == d else 0 for d in "xyz"]
-            return _state(r.shape, np.where(post, 3.857143, 1 + 0.2 * np.sin(5 * r)), *vel,
-                          np.where(post, 10.33333, 1))
+            return _state(r, xp.where(post, 3.857143, 1 + 0.2 * xp.sin(5 * r)), *vel,
+                          xp.where(post, 10.33333, 1))
 
         return f
 
@@ -132,10 +140,12 @@ class KelvinHelmholtz2D(InitialCondition):
 
     def base_ic(self, sigma=0.05 * np.sqrt(2), w0=0.1):
         def f(x, y=None, z=None):
+            xp = of(x)
             band = (y > 0.25) & (y < 0.75)
-            g = np.exp(-np.square(y - 0.25) / (2 * sigma * sigma)) + np.exp(-np.square(y - 0.75) / (2 * sigma * sigma))
-            return _state(band.shape, np.where(band, 2, 1), np.where(band, 0.5, -0.5),
-                          w0 * np.sin(4 * np.pi * x) * g, 0, 2.5)
+            g = xp.exp(xp.div(-xp.square(y - 0.25), 2 * sigma * sigma)) + xp.exp(
+                xp.div(-xp.square(y - 0.75), 2 * sigma * sigma))
+            return _state(band, xp.where(band, 2, 1), xp.where(band, 0.5, -0.5),
+                          w0 * xp.sin(4 * xp.pi * x) * g, 0, 2.5)
 
         return f
 
@@ -155,11 +165,12 @@ class KelvinHelmholtzNoise2D(InitialCondition):
         (x0, x1), (y0, y1) = domain
 
         def f(x, y=None, z=None):
-            ix = np.clip(np.floor((x - x0) / (x1 - x0) * n[0]).astype(int), 0, n[0] - 1)
-            iy = np.clip(np.floor((y - y0) / (y1 - y0) * n[1]).astype(int), 0, n[1] - 1)
-            band = np.abs(y - 0.5) < 0.25
-            return _state(band.shape, np.where(band, 2.0, 1.0), np.where(band, 0.5, -0.5),
-                          0.01 * np.sin(4 * np.pi * x) + noise[ix, iy], 0.0, 2.5)
+            xp = of(x)
+            ix = xp.clip(xp.asint(xp.floor(xp.div(x - x0, x1 - x0) * n[0])), 0, n[0] - 1)
+            iy = xp.clip(xp.asint(xp.floor(xp.div(y - y0, y1 - y0) * n[1])), 0, n[1] - 1)
+            band = xp.abs(y - 0.5) < 0.25
+            return _state(band, xp.where(band, 2.0, 1.0), xp.where(band, 0.5, -0.5),
+                          0.01 * xp.sin(4 * xp.pi * x) + xp.lookup(noise, (ix, iy)), 0.0, 2.5)
 
         return f
 
@@ -181,8 +192,9 @@ class FourQuadrant2D(InitialCondition):
         vy = rng.uniform(-1, 1, size=4)
 
         def f(x, y=None, z=None):
-            q = (x >= xs).astype(int) + 2 * (y >= ys).astype(int)
-            return _state(q.shape, rho[q], vx[q], vy[q], 0.0, P[q])
+            xp = of(x)
+            q = xp.asint(x >= xs) + 2 * xp.asint(y >= ys)
+            return _state(q, xp.lookup(rho, q), xp.lookup(vx, q), xp.lookup(vy, q), 0.0, xp.lookup(P, q))
 
         return f
 
@@ -194,25 +206,26 @@ class ShockTube(InitialCondition):
                 vx_in_out=(0, 0), vy_in_out=(0, 0), vz_in_out=(0, 0), mode="tube", x_cube=None, y_cube=None,
                 z_cube=None):
         def f(x, y=None, z=None):
+            xp = of(x)
             if mode == "tube":
                 c = (center,) if isinstance(center, Number) else tuple(center)
                 if len(c) != len(dims):
                     raise ValueError("center must have the same length as dims")
-                rsq = np.zeros_like(x)
+                rsq = xp.zeros_like(x)
                 for d, cd in zip(dims, c):
                     rsq = rsq + ({"x": x, "y": y, "z": z}[d] - cd) ** 2
                 inside = rsq <= radius**2
             elif mode == "cube":
                 if x_cube is None and y_cube is None and z_cube is None:
                     raise ValueError("at least one cube dimension must be specified")
-                inside = np.ones_like(x, dtype=bool)
+                inside = xp.mask_like(x)
                 for c, rng in zip((x, y, z), (x_cube, y_cube, z_cube)):
                     if rng is not None:
                         inside &= (c >= rng[0]) & (c <= rng[1])
             else:
                 raise ValueError(f"unknown mode {mode}")
-            return _state(x.shape, np.where(inside, *rho_in_out), np.where(inside, *vx_in_out),
-                          np.where(inside, *vy_in_out), np.where(inside, *vz_in_out), np.where(inside, *P_in_out))
+            return _state(x, xp.where(inside, *rho_in_out), xp.where(inside, *vx_in_out),
+                          xp.where(inside, *vy_in_out), xp.where(inside, *vz_in_out), xp.where(inside, *P_in_out))
 
         return f
 
@@ -227,12 +240,13 @@ class SedovBlast(InitialCondition):
 
     def base_ic(self, mode="corner", dims="xy", rho0=1.0, E0=1e-5, E1=1.0):
         def f(x, y=None, z=None):
+            xp = of(x)
             nx, ny, nz = x.shape
             emax = E1
             for d, c, axis in (("x", x, 0), ("y", y, 1), ("z", z, 2)):
                 if d in dims:
-                    emax /= 2 * np.mean(np.diff(c, axis=axis))
-            out = _state(x.shape, rho0, 0, 0, 0, E0)
+                    emax /= 2 * xp.diff_mean(c, axis)
+            out = _state(x, rho0, 0, 0, 0, E0)
             if mode == "corner":
                 out[4, 0, 0, 0] = emax
             elif mode == "center":
@@ -253,7 +267,7 @@ class ArrayIC(InitialCondition):
         arr = np.asarray(array, dtype=np.float64)
 
         def f(x, y=None, z=None):
-            return arr[:5]
+            return arr[:5] if of(x) is of(arr) else of(x).asarray(arr[:5], like=x)
 
         return f
 
@@ -261,8 +275,8 @@ class ArrayIC(InitialCondition):
         arr = np.asarray(self.kwargs.get("array", self.args[0] if self.args else None), dtype=np.float64)
 
         def ic_func(x, y, z):
-            if arr.shape[1:] != np.shape(x):
-                raise ValueError(f"array shape {arr.shape[1:]} does not match the mesh {np.shape(x)}")
-            return arr.copy()
+            if arr.shape[1:] != tuple(np.shape(x)):
+                raise ValueError(f"array shape {arr.shape[1:]} does not match the mesh {tuple(np.shape(x))}")
+            return arr.copy() if of(x) is of(arr) else of(x).asarray(arr, like=x)
 
         return ic_func

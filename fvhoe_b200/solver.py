@@ -108,6 +108,7 @@ class EulerSolver(ODE):
         precision: str = "fp64",
         log_troubles: bool = True,
         kernel_path: str = "auto",
+        ic_on_device: bool = False,
     ):
         if backend is None:
             backend = os.environ.get("FVHOE_BACKEND", "cuda")
@@ -132,6 +133,7 @@ class EulerSolver(ODE):
         self.snapshots_as_fv_averages = snapshots_as_fv_averages
         self.fixed_primitive_variables = fixed_primitive_variables
         self.slab_buffer_size = slab_buffer_size
+        self.ic_on_device = bool(ic_on_device)
         if riemann_solver not in _capi.RIEMANN:
             raise TypeError(f"Invalid Riemann solver {riemann_solver}")
         self._init_mesh(x, y, z, nx, ny, nz, px, py, pz, CFL, fixed_dt)
@@ -186,11 +188,33 @@ class EulerSolver(ODE):
         self.nvars = hs.nvars
         self.w0, self.u0, self.u0_fv = _ic_functions(w0, hs, w0_passives, conservative_ic, fv_ic, self.gamma, self.h,
                                                      self.p)
-        u0 = np.ascontiguousarray(self.u0_fv(self.X, self.Y, self.Z), dtype=np.float64)
         self._ode_init(progress_bar)
         self.am = ArrayManager(backend="cuda")
-        self.am.add("u", u0)
+        if self.ic_on_device:
+            self.am.add_device("u", self._device_initial_state())
+        else:
+            self.am.add("u", np.ascontiguousarray(self.u0_fv(self.X, self.Y, self.Z), dtype=np.float64))
         self.f_evaluation_count = 0
+
+    def _device_initial_state(self):
+        """The FV-averaged initial state evaluated on the device: the same
+        quadrature over the same mesh coordinates (uploaded from the host), with
+        the initial condition's own array code running on torch tensors
+        (array_ns). Library initial conditions support it; an initial condition
+        written for numpy arrays only is refused."""
+        import torch
+
+        dev = torch.device(self.am.device)
+        X, Y, Z = torch.meshgrid(*(torch.from_numpy(np.ascontiguousarray(c)).to(dev) for c in (self.x, self.y, self.z)),
+                                 indexing="ij")
+        try:
+            u0 = self.u0_fv(X, Y, Z)
+        except (TypeError, AttributeError, RuntimeError) as exc:
+            raise TypeError("ic_on_device needs an initial condition written against fvhoe_b200.array_ns "
+                            f"(the library's are); this one failed on device tensors: {exc}") from exc
+        if not isinstance(u0, torch.Tensor):
+            raise TypeError("ic_on_device: the initial condition returned a host array")
+        return u0.to(dtype=torch.float64).contiguous()
 
     def _init_boundary_conditions(self, bc):
         if bc is None:

@@ -254,3 +254,42 @@ def test_snapshot_list_settles_before_reads_and_pickles_as_a_list():
     back = pickle.loads(pickle.dumps(log))
     assert type(back) is list and back == [{"t": 0.0}, {"t": 0.5}]
     assert type(log.copy()) is list
+
+
+@pytest.mark.parametrize("name,kw,exact", [
+    ("Square", dict(dims="xy"), True),
+    ("Shock1D", dict(), True),
+    ("DoubleShock1D", dict(), True),
+    ("ShockTube", dict(dims="xy", center=(0.5, 0.5), radius=0.3), True),
+    ("ShockTube", dict(mode="cube", x_cube=(0.2, 0.6), y_cube=(0.3, 0.9)), True),
+    ("FourQuadrant2D", dict(seed=7), True),
+    ("SedovBlast", dict(mode="corner", dims="xy"), True),
+    ("Sinus", dict(dims="xy"), False),
+    ("ShuOsher1D", dict(), False),
+    ("KelvinHelmholtz2D", dict(), False),
+    ("KelvinHelmholtzNoise2D", dict(n=(24, 20), seed=3), False),
+])
+def test_initial_conditions_evaluate_on_torch_tensors(name, kw, exact):
+    """The library's initial conditions and the FV quadrature run unchanged on
+    torch tensors (the device path of EulerSolver(ic_on_device=True), here on
+    CPU tensors): the same state as on numpy arrays, bit for bit unless the
+    condition uses sin or exp (whose last bit may differ)."""
+    import torch
+
+    import fvhoe_b200.initial_conditions as ic
+    from fvhoe_b200.fv import fv_uniform_meshgen
+    from fvhoe_b200.hydro import HydroState
+    from fvhoe_b200.solver import _ic_functions
+
+    n, p = (24, 20, 1), (5, 5, 0)
+    h = (1 / 24, 1 / 20, 1.0)
+    cons = name == "SedovBlast"
+    _, _, u0_fv = _ic_functions(getattr(ic, name)(**kw), HydroState(), None, cons, cons, 1.4, h, p)
+    X, Y, Z = fv_uniform_meshgen(n)
+    host = u0_fv(X, Y, Z)
+    dev = u0_fv(*(torch.from_numpy(a) for a in (X, Y, Z)))
+    assert isinstance(dev, torch.Tensor) and dev.dtype == torch.float64
+    if exact:
+        assert np.array_equal(dev.numpy(), host)
+    else:
+        assert np.allclose(dev.numpy(), host, rtol=1e-14, atol=1e-15)

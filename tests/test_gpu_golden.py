@@ -179,3 +179,33 @@ def test_snapshots_copied_asynchronously_equal_settled_ones(tmp_path):
     back.snapshot_dir = lazy.snapshot_dir
     assert back.read_snapshots()
     assert all(np.array_equal(a["w"], b["w"]) for a, b in zip(lazy.snapshots, back.snapshots))
+
+
+@pytest.mark.parametrize("ic,exact", [("FourQuadrant2D", True), ("KelvinHelmholtzNoise2D", False)])
+def test_initial_state_averaged_on_the_device(ic, exact):
+    """EulerSolver(ic_on_device=True) averages the initial condition on the
+    device: the same state as the host path (bit for bit without sin/exp), and
+    a refusal for an initial condition written for numpy arrays only."""
+    import fvhoe_b200.initial_conditions as ics
+    from fvhoe_b200 import EulerSolver
+
+    n = (200, 136)
+    w0 = ics.FourQuadrant2D(seed=4) if ic == "FourQuadrant2D" else ics.KelvinHelmholtzNoise2D(n=n, seed=2)
+    kw = dict(w0=w0, nx=n[0], ny=n[1], px=7, py=7, gamma=1.4, a_posteriori_slope_limiting=True, progress_bar=False)
+    host = EulerSolver(**kw)
+    dev = EulerSolver(ic_on_device=True, **kw)
+    a, b = host.am.get_numpy("u"), dev.am.get_numpy("u")
+    if exact:
+        assert np.array_equal(a, b)
+    else:
+        assert np.allclose(a, b, rtol=1e-14, atol=1e-15)
+    host.ssprk3(n=2)
+    dev.ssprk3(n=2)
+    assert np.allclose(host.am.get_numpy("u"), dev.am.get_numpy("u"), rtol=1e-12, atol=1e-13)
+
+    class NumpyOnly(ics.InitialCondition):
+        def base_ic(self):
+            return lambda x, y=None, z=None: np.stack([np.ones_like(x)] * 5)
+
+    with pytest.raises(TypeError):
+        EulerSolver(w0=NumpyOnly(), nx=16, ny=16, ic_on_device=True, progress_bar=False)
