@@ -381,8 +381,9 @@ __device__ __forceinline__ void reduce_keys_and_publish(unsigned long long cfl_k
 // Tile functions: the body of each kernel for the tile (bx, by) (bx along Y,
 // by along X), so that one-problem launches (one tile per block) and the
 // batched ensemble (blocks looping over the tiles of many problems) share it.
-template <typename Tc, int P, int TX, int TY, int KC, bool REDUCE>
-__device__ __forceinline__ void tile2_primitives(const double* __restrict__ u, Geo g, V2<Tc> W, int gw_out,
+// Tin: double for the stage input, the compute type for the candidate
+template <typename Tc, int P, int TX, int TY, int KC, bool REDUCE, typename Tin = double>
+__device__ __forceinline__ void tile2_primitives(const Tin* __restrict__ u, Geo g, V2<Tc> W, int gw_out,
                                                  Rule<Tc, KC> c, Rule<Tc, KC> t, Phys<Tc> ph, ReduceSpec rs,
                                                  Scalars* __restrict__ sc, int bx, int by, unsigned char* smem_raw) {
   using D = PrimsDims<Tc, P, TX, TY>;
@@ -426,12 +427,13 @@ __device__ __forceinline__ void tile2_primitives(const double* __restrict__ u, G
   if constexpr (REDUCE) reduce_keys_and_publish(cfl_key, kmax, kmin, rs, sc);
 }
 
-template <typename Tc, int P, int TX, int TY, int KC, bool REDUCE>
+template <typename Tc, int P, int TX, int TY, int KC, bool REDUCE, typename Tin = double>
 __global__ void __launch_bounds__(256)
-    k2_primitives(const double* __restrict__ u, Geo g, V2<Tc> W, int gw_out, Rule<Tc, KC> c, Rule<Tc, KC> t,
+    k2_primitives(const Tin* __restrict__ u, Geo g, V2<Tc> W, int gw_out, Rule<Tc, KC> c, Rule<Tc, KC> t,
                   Phys<Tc> ph, ReduceSpec rs, Scalars* __restrict__ sc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  tile2_primitives<Tc, P, TX, TY, KC, REDUCE>(u, g, W, gw_out, c, t, ph, rs, sc, blockIdx.x, blockIdx.y, smem_raw);
+  tile2_primitives<Tc, P, TX, TY, KC, REDUCE, Tin>(u, g, W, gw_out, c, t, ph, rs, sc, blockIdx.x, blockIdx.y,
+                                                   smem_raw);
 }
 
 // ---------------------------------------------------------------------------
@@ -719,22 +721,19 @@ __global__ void __launch_bounds__(256, sizeof(Tc) == 4 ? 4 : 3)
 // k2_detect: W* of u* on the tile and 3 ghosts, then the detection of the
 // tile's cells against W (global, >= 3 ghosts).
 // ---------------------------------------------------------------------------
-template <typename Tc, int P, int TX, int TY, int KC>
-__device__ __forceinline__ void tile2_detect(const Tc* __restrict__ ustar, Geo g, V2<const Tc> W, Rule<Tc, KC> c,
-                                             Rule<Tc, KC> t, Phys<Tc> ph, DetectSpec ds, Scalars* __restrict__ sc,
+// Troubled-cell detection of the tile's cells (fvhoe/slope_limiting.py:87-244)
+// from W* on [x0-3, x0+TX+3) x [y0-3, y0+TY+3) in A (row stride OYS) and W
+// (global, >= 3 ghosts), staged into the free buffer B (BCAP elements).
+template <typename Tc, int TX, int TY, int OYS, int BCAP>
+__device__ __forceinline__ void detect_cells(const Tc* __restrict__ A, Tc* __restrict__ B, const Geo& g,
+                                             const V2<const Tc>& W, const DetectSpec& ds, Scalars* __restrict__ sc,
                                              uint8_t* __restrict__ trouble, double* __restrict__ log_trouble,
-                                             double* __restrict__ log_nad, double* __restrict__ log_pad, int bx,
-                                             int by, unsigned char* smem_raw) {
-  constexpr int OX = TX + 6, OY = TY + 6;
-  using D = PrimsDims<Tc, P, OX, OY>;
-  Tc* A = reinterpret_cast<Tc*>(smem_raw);
-  Tc* B = A + D::A;
-  const int x0 = by * TX, y0 = bx * TY;
-  primitives_tile<Tc, P, OX, OY, KC>(ustar, g, x0 - 3, y0 - 3, A, B, c, t, ph);
-  // A now holds W* on [x0-3, x0+TX+3) x [y0-3, y0+TY+3); B is free: stage W on
-  // [x0-1, x0+TX+1) x [y0-1, y0+TY+1) there for the 3x3 box extrema
+                                             double* __restrict__ log_nad, double* __restrict__ log_pad, int x0,
+                                             int y0) {
+  constexpr int OX = TX + 6;
+  // stage W on [x0-1, x0+TX+1) x [y0-1, y0+TY+1) in B for the 3x3 box extrema
   constexpr int WX = TX + 2, WY = TY + 2;
-  static_assert(WX * WY * 5 <= D::B, "W tile must fit in the second buffer");
+  static_assert(WX * WY * 5 <= BCAP, "W tile must fit in the second buffer");
   Tc* Wt = B;
   for (int i = threadIdx.x; i < WX * WY; i += blockDim.x) {
     const int r = i / WY, q = i - r * WY;
@@ -775,7 +774,7 @@ __device__ __forceinline__ void tile2_detect(const Tc* __restrict__ ustar, Geo g
           big = fmax(big, xv);
           small = fmin(small, xv);
         }
-      const Tc* ps = A + (v * OX + r + 3) * D::OYS + q + 3;
+      const Tc* ps = A + (v * OX + r + 3) * OYS + q + 3;
       const Tc xs = ps[0];
       Tc ind;
       bool tv;
@@ -793,7 +792,7 @@ __device__ __forceinline__ void tile2_detect(const Tc* __restrict__ ustar, Geo g
       if (tv && ds.sed) {
         Tc line[7];
 #pragma unroll
-        for (int m = 0; m < 7; ++m) line[m] = ps[(m - 3) * D::OYS];
+        for (int m = 0; m < 7; ++m) line[m] = ps[(m - 3) * OYS];
         bool below = sed_line_below_one(line, sed_eps);
         if (!below) {
 #pragma unroll
@@ -827,6 +826,22 @@ __device__ __forceinline__ void tile2_detect(const Tc* __restrict__ ustar, Geo g
 }
 
 template <typename Tc, int P, int TX, int TY, int KC>
+__device__ __forceinline__ void tile2_detect(const Tc* __restrict__ ustar, Geo g, V2<const Tc> W, Rule<Tc, KC> c,
+                                             Rule<Tc, KC> t, Phys<Tc> ph, DetectSpec ds, Scalars* __restrict__ sc,
+                                             uint8_t* __restrict__ trouble, double* __restrict__ log_trouble,
+                                             double* __restrict__ log_nad, double* __restrict__ log_pad, int bx,
+                                             int by, unsigned char* smem_raw) {
+  constexpr int OX = TX + 6, OY = TY + 6;
+  using D = PrimsDims<Tc, P, OX, OY>;
+  Tc* A = reinterpret_cast<Tc*>(smem_raw);
+  Tc* B = A + D::A;
+  const int x0 = by * TX, y0 = bx * TY;
+  primitives_tile<Tc, P, OX, OY, KC>(ustar, g, x0 - 3, y0 - 3, A, B, c, t, ph);
+  // A now holds W* on [x0-3, x0+TX+3) x [y0-3, y0+TY+3); B is free
+  detect_cells<Tc, TX, TY, D::OYS, D::B>(A, B, g, W, ds, sc, trouble, log_trouble, log_nad, log_pad, x0, y0);
+}
+
+template <typename Tc, int P, int TX, int TY, int KC>
 __global__ void __launch_bounds__(256)
     k2_detect(const Tc* __restrict__ ustar, Geo g, V2<const Tc> W, Rule<Tc, KC> c, Rule<Tc, KC> t, Phys<Tc> ph,
               DetectSpec ds, Scalars* __restrict__ sc, uint8_t* __restrict__ trouble, double* __restrict__ log_trouble,
@@ -834,6 +849,51 @@ __global__ void __launch_bounds__(256)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   tile2_detect<Tc, P, TX, TY, KC>(ustar, g, W, c, t, ph, ds, sc, trouble, log_trouble, log_nad, log_pad, blockIdx.x,
                                   blockIdx.y, smem_raw);
+}
+
+// Detection from a precomputed W*: the primitive kernel run on the candidate
+// over the 3-ghost box (Wst) replaces the W* tile that tile2_detect computes
+// on each tile plus its 3-cell ring; the cells and results are the same.
+template <typename Tc, int TX, int TY>
+struct DetectStagedDims {
+  static constexpr int VW = VecW<Tc>::value;
+  static constexpr int OX = TX + 6, OY = TY + 6, OYS = (OY + VW - 1) / VW * VW;
+  static constexpr int A = OX * OYS * 5 + 16;         // W* tile
+  static constexpr int B = (TX + 2) * (TY + 2) * 5 + 16;  // W tile
+  static constexpr int TOTAL = A + B;                 // elements of the compute type
+};
+
+template <typename Tc, int TX, int TY>
+__device__ __forceinline__ void tile2_detect_staged(V2<const Tc> Wst, Geo g, V2<const Tc> W, DetectSpec ds,
+                                                    Scalars* __restrict__ sc, uint8_t* __restrict__ trouble,
+                                                    double* __restrict__ log_trouble, double* __restrict__ log_nad,
+                                                    double* __restrict__ log_pad, int bx, int by,
+                                                    unsigned char* smem_raw) {
+  using D = DetectStagedDims<Tc, TX, TY>;
+  Tc* A = reinterpret_cast<Tc*>(smem_raw);
+  Tc* B = A + D::A;
+  const int x0 = by * TX, y0 = bx * TY;
+  // W* on [x0-3, x0+TX+3) x [y0-3, y0+TY+3), clamped into the 3-ghost box
+  // (points past it feed only cells outside the grid)
+  for (int i = threadIdx.x; i < D::OX * D::OY; i += blockDim.x) {
+    const int r = i / D::OY, q = i - r * D::OY;
+    const int x = min(x0 - 3 + r, g.nx + 2), y = min(y0 - 3 + q, g.ny + 2);
+    const Tc* p = Wst.p + Wst.at(x, y);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) A[(v * D::OX + r) * D::OYS + q] = p[v * Wst.vs];
+  }
+  // detect_cells stages W and synchronises before the first read of either tile
+  detect_cells<Tc, TX, TY, D::OYS, D::B>(A, B, g, W, ds, sc, trouble, log_trouble, log_nad, log_pad, x0, y0);
+}
+
+template <typename Tc, int TX, int TY>
+__global__ void __launch_bounds__(256, 6)
+    k2_detect_staged(V2<const Tc> Wst, Geo g, V2<const Tc> W, DetectSpec ds, Scalars* __restrict__ sc,
+                     uint8_t* __restrict__ trouble, double* __restrict__ log_trouble, double* __restrict__ log_nad,
+                     double* __restrict__ log_pad) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  tile2_detect_staged<Tc, TX, TY>(Wst, g, W, ds, sc, trouble, log_trouble, log_nad, log_pad, blockIdx.x, blockIdx.y,
+                                  smem_raw);
 }
 
 // ---------------------------------------------------------------------------

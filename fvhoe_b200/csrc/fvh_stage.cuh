@@ -668,16 +668,29 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     ds.force_trouble = cfg.force_trouble;
     ds.log_mode = cfg.log_troubles ? c.log_mode : 0;
     ds.log_div = ds.log_mode ? c.log_div : 0.0;
-    using D = f2::PrimsDims<Tc, P, T::DX + 6, T::DY + 6>;
-    const size_t smem = (size_t)(D::A + D::B) * sizeof(Tc);
-    auto kern = f2::k2_detect<Tc, P, T::DX, T::DY, KC>;
+    // W* of the candidate over its 3-ghost box, once per cell: the primitive
+    // kernel on u* (no reductions)
+    const f2::V2<Tc> Wst = f2::make_v2((Tc*)h->Ws, g.nx, g.ny, 3);
+    {
+      using DP = f2::PrimsDims<Tc, P, T::PX, T::PY>;
+      const size_t smemp = (size_t)(DP::A + DP::B) * sizeof(Tc);
+      auto kp = f2::k2_primitives<Tc, P, T::PX, T::PY, KC, false, Tc>;
+      set_smem((const void*)kp, smemp);
+      const dim3 gp((g.ny + 6 + T::PY - 1) / T::PY, (g.nx + 6 + T::PX - 1) / T::PX);
+      LaunchScope scope(KK_CENTRE, cells * 5 * 2.0 * sizeof(Tc), s);
+      kp<<<gp, 256, smemp, s>>>((const Tc*)h->Us, g, Wst, 3, crule, trule, ph, ReduceSpec{}, h->sc);
+      if ((st = set_cuda_error(h, "fused candidate primitives"))) return st;
+    }
+    using D = f2::DetectStagedDims<Tc, T::DX, T::DY>;
+    const size_t smem = (size_t)D::TOTAL * sizeof(Tc);
+    auto kern = f2::k2_detect_staged<Tc, T::DX, T::DY>;
     set_smem((const void*)kern, smem);
     const dim3 grid((g.ny + T::DY - 1) / T::DY, (g.nx + T::DX - 1) / T::DX);
-    // candidate and W in (compute type), flags out, trouble-log sums in and out
+    // W* and W in (compute type), flags out, trouble-log sums in and out
     LaunchScope scope(KK_DETECT, cells * (10.0 * sizeof(Tc) + 1 + (ds.log_mode ? 48.0 : 0.0)), s);
     f2::V2<const Tc> Wc{(const Tc*)h->W, h->gW, g.ny + 2 * h->gW, (g.nx + 2 * h->gW) * (g.ny + 2 * h->gW)};
-    kern<<<grid, 256, smem, s>>>((const Tc*)h->Us, g, Wc, crule, trule, ph, ds, h->sc, h->trouble, h->logs[0], h->logs[1],
-                                 h->logs[2]);
+    f2::V2<const Tc> Wsc{Wst.p, Wst.g, Wst.sx, Wst.vs};
+    kern<<<grid, 256, smem, s>>>(Wsc, g, Wc, ds, h->sc, h->trouble, h->logs[0], h->logs[1], h->logs[2]);
     if ((st = set_cuda_error(h, "fused detect"))) return st;
   }
   if (pred && (st = mlp_count_stage(h, s))) return st;
