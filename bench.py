@@ -424,23 +424,23 @@ def predictor_leg(args, stream, sp):
     }
 
 
-def ensemble_members(count, seed=2024):
+def ensemble_members(count, seed=2024, side=None):
     """The batched-ensemble workload: square grids of side drawn uniformly from
-    {128, 192, ..., 1024}, each a four-quadrant Riemann problem with its own
-    seeded split point and states."""
+    {128, 192, ..., 1024} (or all of one side), each a four-quadrant Riemann
+    problem with its own seeded split point and states."""
     import numpy as np
 
     from fvhoe_b200 import FourQuadrant2D
 
     rng = np.random.default_rng(seed)
-    sides = rng.choice(np.arange(128, 1025, 64), size=count)
+    sides = rng.choice(np.arange(128, 1025, 64), size=count) if side is None else np.full(count, side)
     return [dict(w0=FourQuadrant2D(seed=1000 + q), nx=int(s), ny=int(s)) for q, s in enumerate(sides)]
 
 
 ENSEMBLE_KW = dict(gamma=1.4, riemann_solver="hllc", CFL=0.8, a_posteriori_slope_limiting=True, NAD=1e-5)
 
 
-def ensemble_leg(args, stream):
+def ensemble_leg(args, stream, members=None, label=None):
     """256 independent four-quadrant problems (p=3, HLLC, SSP-RK3, CFL 0.8,
     outflow, a-posteriori NAD 1e-5 + PAD + SED, FP32 with FP64 stage
     accumulation), target t_end = 0.2 each: autotuned tile shape and blocks per
@@ -451,7 +451,9 @@ def ensemble_leg(args, stream):
 
     from fvhoe_b200 import BoundaryCondition, Ensemble, EulerSolver
 
-    members = ensemble_members(args.ens_members)
+    if members is None:
+        members = ensemble_members(args.ens_members)
+        label = "square sides uniform in {128..1024 step 64}"
     kw = dict(ENSEMBLE_KW, bc=BoundaryCondition(x="outflow", y="outflow"))
     t0 = time.perf_counter()
     ens = Ensemble(members, px=3, precision="fp32", **kw)
@@ -488,12 +490,16 @@ def ensemble_leg(args, stream):
         m = members[q]
         s = EulerSolver(w0=m["w0"], nx=m["nx"], ny=m["ny"], px=3, py=3, precision="fp32", progress_bar=False,
                         log_troubles=False, **kw)
-        s.ssprk3(n=args.warmup)
+        # the stepper alone, like the ensemble (integrate() would add two snapshots per call)
+        s.integrator = "ssprk3"
+        for _ in range(args.warmup):
+            s.take_step()
         torch.cuda.synchronize()
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        s.ssprk3(n=args.ens_steps)
+        for _ in range(args.ens_steps):
+            s.take_step()
         b.record(stream)
         torch.cuda.synchronize()
         single_ms += a.elapsed_time(b)
@@ -501,14 +507,15 @@ def ensemble_leg(args, stream):
         del s
     single_value = single_updates / (single_ms / 1e3) / 1e6
     return {
-        "config": f"{len(members)} four-quadrant Riemann problems, square sides uniform in {{128..1024 step 64}} "
+        "config": f"{len(members)} four-quadrant Riemann problems, {label} "
                   f"({cells} cells), p=3, HLLC, SSP-RK3, CFL 0.8, outflow, NAD 1e-5 + PAD + SED, FP32 with FP64 "
                   "stage accumulation, t_end = 0.2 each",
         "value": value, "unit": UNIT, "steps": args.ens_steps, "ms_per_step": ms / args.ens_steps,
         "cell_updates": int(updates), "active_after": after["active"], "nonfinite": after["nonfinite"],
         "autotune": tune, "graph": graph, "device_bytes": nbytes, "setup_seconds": t_setup,
         "one_at_a_time": {"members": len(pick), "value": single_value,
-                          "path": "EulerSolver.ssprk3, one fused-path step per member and step (dt read back)"},
+                          "path": "EulerSolver.take_step (SSP-RK3), one fused-path step per member and step, "
+                                  "dt read back"},
         "batching_gain": value / single_value,
     }
 
@@ -656,6 +663,9 @@ def run_ours(args):
             torch.cuda.empty_cache()
             try:
                 line["batched_ensemble"] = ensemble_leg(args, stream)
+                # where batching pays: many small members, launch- and host-bound one at a time
+                line["batched_ensemble"]["small_members"] = ensemble_leg(
+                    args, stream, ensemble_members(args.ens_members, side=128), "all of side 128")
             except Exception as exc:
                 line["batched_ensemble"] = {"error": f"{type(exc).__name__}: {exc}"}
         print(json.dumps(line), flush=True)
