@@ -541,7 +541,8 @@ template <typename Tc>
 struct FusedTiles;
 template <>
 struct FusedTiles<float> {
-  static constexpr int PX = 32, PY = 32;  // primitives (register-limited to 3 blocks/SM either way)
+  static constexpr int PX = 32, PY = 32;  // primitives of the stage input
+  static constexpr int SX = 24, SY = 32;  // primitives of the candidate (W* over the 3-ghost box; 4 blocks/SM)
   static constexpr int FX = 16, FY = 32;  // fluxes
   static constexpr int DX = 16, DY = 32;  // detection
   static constexpr int EX = 16, EY = 32;  // fallback + final
@@ -549,6 +550,7 @@ struct FusedTiles<float> {
 template <>
 struct FusedTiles<double> {
   static constexpr int PX = 16, PY = 32;
+  static constexpr int SX = 16, SY = 32;
   static constexpr int FX = 8, FY = 32;
   static constexpr int DX = 8, DY = 32;
   static constexpr int EX = 8, EY = 32;
@@ -672,11 +674,11 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     // kernel on u* (no reductions)
     const f2::V2<Tc> Wst = f2::make_v2((Tc*)h->Ws, g.nx, g.ny, 3);
     {
-      using DP = f2::PrimsDims<Tc, P, T::PX, T::PY>;
+      using DP = f2::PrimsDims<Tc, P, T::SX, T::SY>;
       const size_t smemp = (size_t)(DP::A + DP::B) * sizeof(Tc);
-      auto kp = f2::k2_primitives<Tc, P, T::PX, T::PY, KC, false, Tc>;
+      auto kp = f2::k2_primitives<Tc, P, T::SX, T::SY, KC, false, Tc>;
       set_smem((const void*)kp, smemp);
-      const dim3 gp((g.ny + 6 + T::PY - 1) / T::PY, (g.nx + 6 + T::PX - 1) / T::PX);
+      const dim3 gp((g.ny + 6 + T::SY - 1) / T::SY, (g.nx + 6 + T::SX - 1) / T::SX);
       LaunchScope scope(KK_CENTRE, cells * 5 * 2.0 * sizeof(Tc), s);
       kp<<<gp, 256, smemp, s>>>((const Tc*)h->Us, g, Wst, 3, crule, trule, ph, ReduceSpec{}, h->sc);
       if ((st = set_cuda_error(h, "fused candidate primitives"))) return st;
