@@ -1,4 +1,4 @@
-// Fused 2D stage: four shared-memory-tiled kernels per stage instead of the
+// Fused 2D stage: five shared-memory-tiled launches per stage instead of the
 // generic path's ~21 passes, for problems with two active axes, five
 // variables and the same degree p (1..8) on both axes.
 //
@@ -12,8 +12,10 @@
 //                  (fvhoe/solver.py:753-792, fvhoe/hydro.py:270-294)
 //   k2_fluxes      X- and Y-face high-order fluxes from W and the candidate
 //                  u* = u + dt L(F) (fvhoe/solver.py:519-651, 677-678)
-//   k2_detect      W* of u* on the tile plus 3 ghosts, then troubled-cell
-//                  detection (fvhoe/slope_limiting.py:87-244)
+//   k2_primitives  on the candidate: W* over [-3, n+3)^2 (no reductions)
+//   k2_detect_staged  troubled-cell detection from the W* and W tiles
+//                  (fvhoe/slope_limiting.py:87-244); the batched ensemble's
+//                  phase computes W* on each tile instead (tile2_detect)
 //   k2_final       MUSCL fallback fluxes at troubled faces, the blend, the flux
 //                  divergence and the Runge-Kutta combination
 //                  (fvhoe/solver.py:710-751, fvhoe/ode.py:245-298)
@@ -718,8 +720,9 @@ __global__ void __launch_bounds__(256, sizeof(Tc) == 4 ? 4 : 3)
 }
 
 // ---------------------------------------------------------------------------
-// k2_detect: W* of u* on the tile and 3 ghosts, then the detection of the
-// tile's cells against W (global, >= 3 ghosts).
+// Detection: detect_cells (shared), tile2_detect (W* computed on the tile and
+// its 3-cell ring, for the ensemble's persistent phase) and the staged form
+// (W* precomputed over the grid, for the one-problem launches).
 // ---------------------------------------------------------------------------
 // Troubled-cell detection of the tile's cells (fvhoe/slope_limiting.py:87-244)
 // from W* on [x0-3, x0+TX+3) x [y0-3, y0+TY+3) in A (row stride OYS) and W
@@ -841,15 +844,6 @@ __device__ __forceinline__ void tile2_detect(const Tc* __restrict__ ustar, Geo g
   detect_cells<Tc, TX, TY, D::OYS, D::B>(A, B, g, W, ds, sc, trouble, log_trouble, log_nad, log_pad, x0, y0);
 }
 
-template <typename Tc, int P, int TX, int TY, int KC>
-__global__ void __launch_bounds__(256)
-    k2_detect(const Tc* __restrict__ ustar, Geo g, V2<const Tc> W, Rule<Tc, KC> c, Rule<Tc, KC> t, Phys<Tc> ph,
-              DetectSpec ds, Scalars* __restrict__ sc, uint8_t* __restrict__ trouble, double* __restrict__ log_trouble,
-              double* __restrict__ log_nad, double* __restrict__ log_pad) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  tile2_detect<Tc, P, TX, TY, KC>(ustar, g, W, c, t, ph, ds, sc, trouble, log_trouble, log_nad, log_pad, blockIdx.x,
-                                  blockIdx.y, smem_raw);
-}
 
 // Detection from a precomputed W*: the primitive kernel run on the candidate
 // over the 3-ghost box (Wst) replaces the W* tile that tile2_detect computes
