@@ -472,11 +472,9 @@ struct FluxDims {
   static constexpr int TOTAL = S0 + S1 + S2;  // elements of the compute type
 };
 
-#ifndef FVH_FLUX_FW
-#define FVH_FLUX_FW 2
-#endif
-// FW: faces per thread in the Riemann phases (1, 2 or 4)
-template <typename Tc, int P, int TX, int TY, int KC, int KF, int FW = (sizeof(Tc) == 4 ? FVH_FLUX_FW : 1)>
+// FW: faces per thread in the Riemann phases (1, 2 or 4): two in FP32, one in
+// FP64, where two faces' FP64 states would cost a block per SM in registers
+template <typename Tc, int P, int TX, int TY, int KC, int KF, int FW = (sizeof(Tc) == 4 ? 2 : 1)>
 __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __restrict__ u, Geo g, V2<Tc> F, V2<Tc> G,
                                              Tc* __restrict__ ustar, Rule<Tc, KC> c, Rule<Tc, KC> t,
                                              Rule<Tc, KF> lrule, Rule<Tc, KF> rrule, Phys<Tc> ph, double cx,
