@@ -43,8 +43,9 @@ class _Numpy:
         return x.astype(int)
 
     @staticmethod
-    def lookup(table, index):
-        """table[index] for a host table and an index array (or tuple of them)."""
+    def lookup(table, index, cache=None):
+        """table[index] for a host table and an index array (or tuple of them);
+        cache (a dict the caller owns) keeps device copies of the table."""
         return np.asarray(table)[index]
 
     @staticmethod
@@ -63,7 +64,6 @@ class _Torch:
         import torch
 
         self.torch = torch
-        self._tables = {}
 
     def _t(self, a, like):
         if isinstance(a, self.torch.Tensor):
@@ -113,14 +113,16 @@ class _Torch:
     def asint(self, x):
         return x.long()
 
-    def lookup(self, table, index):
-        key = (id(table), index[0].device if isinstance(index, tuple) else index.device)
-        t = self._tables.get(key)
-        if t is None or t[0] is not table:
-            dev = key[1]
-            t = (table, self.torch.as_tensor(np.asarray(table), device=dev))
-            self._tables[key] = t
-        return t[1][index]
+    def lookup(self, table, index, cache=None):
+        # the device copy lives in the caller's cache (an initial condition's
+        # closure), so it is freed with the solver that holds that closure
+        dev = index[0].device if isinstance(index, tuple) else index.device
+        t = cache.get(dev) if cache is not None else None
+        if t is None:
+            t = self.torch.as_tensor(np.asarray(table), device=dev)
+            if cache is not None:
+                cache[dev] = t
+        return t[index]
 
     def diff_mean(self, c, axis):
         # numpy's own reduction on the host copy, so the value equals the host path's

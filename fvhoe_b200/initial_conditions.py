@@ -162,6 +162,7 @@ class KelvinHelmholtzNoise2D(InitialCondition):
     def base_ic(self, n: Sequence[int] = (64, 64), seed: int = 0, amplitude: float = 1e-3,
                 domain=((0.0, 1.0), (0.0, 1.0))):
         noise = np.random.default_rng(seed).uniform(-amplitude, amplitude, size=tuple(n[:2]))
+        tables = {}  # device copies of the noise, per device
         (x0, x1), (y0, y1) = domain
 
         def f(x, y=None, z=None):
@@ -170,7 +171,7 @@ class KelvinHelmholtzNoise2D(InitialCondition):
             iy = xp.clip(xp.asint(xp.floor(xp.div(y - y0, y1 - y0) * n[1])), 0, n[1] - 1)
             band = xp.abs(y - 0.5) < 0.25
             return _state(band, xp.where(band, 2.0, 1.0), xp.where(band, 0.5, -0.5),
-                          0.01 * xp.sin(4 * xp.pi * x) + xp.lookup(noise, (ix, iy)), 0.0, 2.5)
+                          0.01 * xp.sin(4 * xp.pi * x) + xp.lookup(noise, (ix, iy), tables), 0.0, 2.5)
 
         return f
 
@@ -190,11 +191,13 @@ class FourQuadrant2D(InitialCondition):
         P = np.exp(rng.uniform(np.log(0.01), np.log(10.0), size=4))
         vx = rng.uniform(-1, 1, size=4)
         vy = rng.uniform(-1, 1, size=4)
+        tables = ({}, {}, {}, {})  # device copies of rho, vx, vy, P, per device
 
         def f(x, y=None, z=None):
             xp = of(x)
             q = xp.asint(x >= xs) + 2 * xp.asint(y >= ys)
-            return _state(q, xp.lookup(rho, q), xp.lookup(vx, q), xp.lookup(vy, q), 0.0, xp.lookup(P, q))
+            return _state(q, xp.lookup(rho, q, tables[0]), xp.lookup(vx, q, tables[1]), xp.lookup(vy, q, tables[2]),
+                          0.0, xp.lookup(P, q, tables[3]))
 
         return f
 
