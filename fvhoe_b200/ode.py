@@ -73,6 +73,14 @@ class SnapshotList(list):
         self._settle()
         return super().count(x)
 
+    def pop(self, *args):
+        self._settle()
+        return super().pop(*args)
+
+    def remove(self, x):
+        self._settle()
+        return super().remove(x)
+
     def __reduce_ex__(self, protocol):
         self._settle()
         return (list, (list(super().__iter__()),))

@@ -254,6 +254,8 @@ def test_snapshot_list_settles_before_reads_and_pickles_as_a_list():
     back = pickle.loads(pickle.dumps(log))
     assert type(back) is list and back == [{"t": 0.0}, {"t": 0.5}]
     assert type(log.copy()) is list
+    n = len(calls)
+    assert log.pop()["t"] == 0.5 and len(calls) == n + 1
 
 
 @pytest.mark.parametrize("name,kw,exact", [
