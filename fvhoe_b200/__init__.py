@@ -12,6 +12,7 @@ from .boundary_conditions import BoundaryCondition
 from .hydro import HydroState, advection_dt
 from .initial_conditions import (
     ArrayIC,
+    DoubleMachReflection2D,
     DoubleShock1D,
     FourQuadrant2D,
     InitialCondition,
@@ -31,6 +32,7 @@ __all__ = [
     "ArrayIC",
     "ArrayManager",
     "BoundaryCondition",
+    "DoubleMachReflection2D",
     "DoubleShock1D",
     "Ensemble",
     "EulerSolver",

@@ -11,7 +11,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libfvh.so")
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 OK = 0
 ERR_CONFIG = -1
@@ -20,7 +20,8 @@ ERR_TIMEOUT = -3
 ERR_NONFINITE = -4
 ERR_ARG = -5
 
-BC = {"periodic": 0, "outflow": 1, "reflective": 2, "free": 3, "dirichlet": 4}
+DMR_Y0 = "special-case-double-mach-reflection-y=0"
+BC = {"periodic": 0, "outflow": 1, "reflective": 2, "free": 3, "dirichlet": 4, DMR_Y0: 5}
 RIEMANN = {"hllc": 0, "llf": 1, "advection_upwind": 2}
 LIMITER = {"minmod": 0, "moncen": 1, None: 2}
 PRECISION = {"fp64": 0, "fp32": 1}
@@ -119,6 +120,7 @@ class FvhConfig(ctypes.Structure):
         ("log_troubles", ctypes.c_int),
         ("device", ctypes.c_int),
         ("kernel_path", ctypes.c_int),
+        ("dmr_split", ctypes.c_int),
     ]
 
 

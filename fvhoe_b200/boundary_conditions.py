@@ -8,6 +8,9 @@ materialised: the CUDA kernels read the interior through per-axis index maps
 repeat), which is what the reference's slab copies produce, and read the
 ghost values of "dirichlet" and "ic" sides from arrays the solver evaluates
 at the reference's slab coordinates (fvhoe/boundary_conditions.py:18-55).
+The low y side may be "special-case-double-mach-reflection-y=0", the wall of
+the double Mach reflection problem (:374-395): free where the ghost column's
+x centre is below 1/6, reflective elsewhere.
 """
 
 from dataclasses import dataclass, field
@@ -15,10 +18,24 @@ from typing import Any, Tuple, Union
 
 import numpy as np
 
-SUPPORTED = ("periodic", "outflow", "reflective", "free", "dirichlet", "ic")
-# the reference's own branch for this kind calls _set_free_bc without its first
-# argument (fvhoe/boundary_conditions.py:382), so it cannot run there either
-NOT_SUPPORTED = ("special-case-double-mach-reflection-y=0",)
+DMR_Y0 = "special-case-double-mach-reflection-y=0"
+SUPPORTED = ("periodic", "outflow", "reflective", "free", "dirichlet", "ic", DMR_Y0)
+
+
+def dmr_split(n, x, y, z, buffer) -> int:
+    """First x index (ghost cells negative) where the double-Mach-reflection
+    wall turns reflective. The reference picks free ghost values where the
+    column's x centre on its low-y slab coordinates (`buffer` cells deep per
+    axis) is below 1/6 (fvhoe/boundary_conditions.py:375-395); the centres
+    increase with the index, so the free columns are a prefix."""
+    from .fv import slab_meshgen
+
+    X = slab_meshgen(n, x, y, z, buffer)["yl"][0][:, 0, 0]
+    free = X < 1 / 6
+    split = free.size if free.all() else int(np.argmin(free))
+    if free[split:].any():
+        raise ValueError("slab x centres are not increasing")
+    return split - buffer[0]
 
 
 @dataclass
@@ -46,19 +63,16 @@ class BoundaryCondition:
                     setattr(self, f"{dim}{suffix}", (value, value))
 
     def kinds(self, active: Tuple[bool, bool, bool]):
-        """(low, high) kinds per axis; raises for kinds the CUDA backend does not provide."""
+        """(low, high) kinds per axis; raises for unknown kinds and misplaced ones."""
         out = []
         for dim, on in zip("xyz", active):
             pair = getattr(self, dim)
             if on:
                 for kind in pair:
-                    if kind in NOT_SUPPORTED:
-                        raise NotImplementedError(
-                            f"boundary '{kind}' on {dim} is not provided by the CUDA backend "
-                            f"(supported: {', '.join(SUPPORTED)})"
-                        )
                     if kind not in SUPPORTED:
                         raise ValueError(f"Unknown bc type '{kind}'")
+                if pair[1] == DMR_Y0 or (pair[0] == DMR_Y0 and dim != "y"):
+                    raise ValueError(f"'{DMR_Y0}' is defined on the low y side only")
                 if pair[1] == "periodic" and pair[0] != "periodic":
                     raise ValueError(f"a periodic high boundary on {dim} needs a periodic low boundary")
                 values = getattr(self, f"{dim}_value")

@@ -140,8 +140,12 @@ int configure(fvh_handle* h, const fvh_config* cfg, std::string& msg) {
     if (!h->active[a]) continue;
     for (int side = 0; side < 2; ++side) {
       const int k = cfg->bc[a][side];
-      if (k < FVH_BC_PERIODIC || k > FVH_BC_DIRICHLET) {
+      if (k < FVH_BC_PERIODIC || k > FVH_BC_DMR_Y0) {
         msg = "unsupported boundary kind";
+        return FVH_ERR_CONFIG;
+      }
+      if (k == FVH_BC_DMR_Y0 && !(a == 1 && side == 0)) {
+        msg = "the double-Mach-reflection boundary is defined on the low y side only";
         return FVH_ERR_CONFIG;
       }
     }
@@ -323,9 +327,11 @@ int allocate(fvh_handle* h) {
   if ((st = alloc(h, (void**)&h->S[1], state))) return st;
   if ((st = alloc(h, (void**)&h->sc, sizeof(fvh::Scalars)))) return st;
   cudaMemset(h->sc, 0, sizeof(fvh::Scalars));
-  // Dirichlet sides: ghost-value arrays (zero until the caller uploads) and their descriptor
-  bool dirichlet = false;
+  // Dirichlet sides: ghost-value arrays (zero until the caller uploads) and their
+  // descriptor, which the double-Mach-reflection wall also needs (its split)
+  bool dirichlet = h->active[1] && h->cfg.bc[1][0] == FVH_BC_DMR_Y0;
   fvh::Slabs& m = h->slab_meta;
+  m.dmr_split = h->cfg.dmr_split;
   for (int a = 0; a < 3; ++a) {
     m.n[a] = h->n[a];
     m.depth[a] = h->active[a] ? h->gW + 2 * h->r[a] : 0;

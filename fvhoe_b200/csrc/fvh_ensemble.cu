@@ -155,9 +155,10 @@ int fvh_ensemble_create(const fvh_config* cfg, int nprob, const int* nx, const i
     }
     for (int a = 0; a < 2; ++a)
       for (int side = 0; side < 2; ++side)
-        if (c.bc[a][side] == FVH_BC_DIRICHLET) {
+        if (c.bc[a][side] == FVH_BC_DIRICHLET || c.bc[a][side] == FVH_BC_DMR_Y0) {
           delete e;
-          return fail(nullptr, FVH_ERR_CONFIG, "ensemble members cannot have Dirichlet boundaries");
+          return fail(nullptr, FVH_ERR_CONFIG,
+                      "ensemble members cannot have Dirichlet or double-Mach-reflection boundaries");
         }
     if (!tmp.active[0] || !tmp.active[1]) {
       delete e;

@@ -25,7 +25,7 @@
 
 namespace fvh {
 
-enum Bc : int { BC_PERIODIC = 0, BC_OUTFLOW = 1, BC_REFLECTIVE = 2, BC_FREE = 3, BC_DIRICHLET = 4 };
+enum Bc : int { BC_PERIODIC = 0, BC_OUTFLOW = 1, BC_REFLECTIVE = 2, BC_FREE = 3, BC_DIRICHLET = 4, BC_DMR_Y0 = 5 };
 
 struct Region {
   int lo[3];
@@ -38,12 +38,16 @@ struct Region {
 // E_b = n_b + 2 pad[b] along the other axes (their ghost layers included).
 // Element (v, i) of a ghost cell i: along a, i_a + depth[a] on the low side and
 // i_a - n_a on the high side; along b, i_b + pad[b].
+// A BC_DMR_Y0 low y side (the double-Mach-reflection wall) has no slab: its
+// ghost cells take free or reflective values by the x index of their column
+// (below dmr_split: free), fvhoe/boundary_conditions.py:374-395.
 struct Slabs {
   int n[3];
   int bc[3][2];
   const double* p[3][2];  // nullptr unless that side is Dirichlet
   int depth[3];
   int pad[3];
+  int dmr_split;
 };
 
 struct Grid {
@@ -194,8 +198,12 @@ __device__ __forceinline__ void dirichlet_core(const Tin* __restrict__ u, const 
       }
       return;
     }
+    // the double-Mach-reflection wall chooses by the column's x index, still
+    // unmapped here because x is resolved last (it was filled first)
+    int lo = sl->bc[a][0];
+    if (lo == BC_DMR_Y0) lo = i[0] < sl->dmr_split ? BC_FREE : BC_REFLECTIVE;
     bool f = false;
-    i[a] = ghost_source(ia, na, sl->bc[a][0], sl->bc[a][1], f);
+    i[a] = ghost_source(ia, na, lo, sl->bc[a][1], f);
     flip[a] = f;
   }
   const int plane = sl->n[0] * sl->n[1] * sl->n[2];

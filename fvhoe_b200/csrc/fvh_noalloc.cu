@@ -85,8 +85,9 @@ int fvh_primitives_noalloc(const fvh_config* cfg, const double* u, double* w, in
   if (h.cfg.device >= kMaxDevices) return set_error(FVH_ERR_CONFIG, "device ordinal too large");
   for (int a = 0; a < 3; ++a)
     for (int side = 0; side < 2; ++side)
-      if (h.active[a] && cfg->bc[a][side] == FVH_BC_DIRICHLET)
-        return set_error(FVH_ERR_CONFIG, "Dirichlet boundaries need a handle (fvh_primitives) for their ghost values");
+      if (h.active[a] && (cfg->bc[a][side] == FVH_BC_DIRICHLET || cfg->bc[a][side] == FVH_BC_DMR_Y0))
+        return set_error(FVH_ERR_CONFIG,
+                         "Dirichlet and double-Mach-reflection boundaries need a handle (fvh_primitives)");
   // per-buffer requirement: the state ghost-filled by 2r on each active axis
   size_t need = (size_t)h.nv;
   for (int a = 0; a < 3; ++a) need *= (size_t)(h.n[a] + (h.active[a] ? 4 * h.r[a] : 0));

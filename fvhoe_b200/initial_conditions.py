@@ -202,6 +202,25 @@ class FourQuadrant2D(InitialCondition):
         return f
 
 
+class DoubleMachReflection2D(InitialCondition):
+    """A Mach-10 shock through x = 1/6 at y = 0, inclined at 60 degrees to the x
+    axis: the shocked state (rho 8, v = (7.145, -4.125), P 116.5) lies left of
+    x - y / tan(pi/3) = 1/6, the gas at rest (rho = gamma, P 1) right of it
+    (fvhoe/initial_conditions.py:369-399). Used with the low-y wall
+    "special-case-double-mach-reflection-y=0"."""
+
+    def base_ic(self, gamma: float = 1.4):
+        tan = np.tan(np.pi / 3)
+
+        def f(x, y=None, z=None):
+            xp = of(x)
+            post = (x - xp.div(y, tan)) < 1 / 6
+            return _state(post, xp.where(post, 8, gamma), xp.where(post, 7.145, 0),
+                          xp.where(post, -8.25 / 2, 0), 0, xp.where(post, 116.5, 1))
+
+        return f
+
+
 class ShockTube(InitialCondition):
     """Inside/outside states of a ball ("tube") or an axis-aligned box ("cube")."""
 

@@ -24,7 +24,7 @@ from typing import Callable, Dict, Iterable, Tuple
 import numpy as np
 
 from .array_management import ArrayManager
-from .boundary_conditions import BoundaryCondition
+from .boundary_conditions import DMR_Y0, BoundaryCondition
 from .fv import fv_average, fv_uniform_meshgen
 from .hydro import HydroState, compute_conservatives
 from .initial_conditions import InitialCondition, Square
@@ -256,6 +256,7 @@ class EulerSolver(ODE):
                 if kind == "ic":
                     kind = "dirichlet"
                 cfg.bc[a][side] = c.BC.get(kind, 0) if kind is not None else 0
+        cfg.dmr_split = self._dmr_split() if self._bc_kinds[1][0] == DMR_Y0 else 0
         cfg.gamma = self.gamma
         cfg.cfl = self.CFL
         cfg.csq_floor = self.csq_floor
@@ -290,6 +291,13 @@ class EulerSolver(ODE):
         cfg.device = int(self.am("u").device.index or 0)
         cfg.kernel_path = c.PATH[self.kernel_path]
         return cfg
+
+    def _dmr_split(self) -> int:
+        from .boundary_conditions import dmr_split
+
+        active = (self.xdim, self.ydim, self.zdim)
+        buffer = tuple(self.slab_buffer_size if on else 0 for on in active)
+        return dmr_split(self.n, self.x_domain, self.y_domain, self.z_domain, buffer)
 
     def _create_handle(self):
         import torch

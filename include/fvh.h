@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define FVH_ABI_VERSION 1
+#define FVH_ABI_VERSION 2
 
 /* status codes */
 #define FVH_OK 0
@@ -48,6 +48,10 @@ extern "C" {
 #define FVH_BC_REFLECTIVE 2 /* mirror, normal momentum negated */
 #define FVH_BC_FREE 3 /* repeat the edge cell */
 #define FVH_BC_DIRICHLET 4 /* ghost values given by the caller ("dirichlet" and "ic") */
+/* "special-case-double-mach-reflection-y=0" (fvhoe/boundary_conditions.py:374-395),
+   low y side only: a ghost column whose x index is below dmr_split repeats the
+   edge cell (free), the others mirror with the y momentum negated (reflective) */
+#define FVH_BC_DMR_Y0 5
 
 /* Riemann solvers (fvhoe/solver.py:185-193) */
 #define FVH_RIEMANN_HLLC 0
@@ -99,6 +103,7 @@ typedef struct fvh_config {
   int log_troubles;  /* 1: keep the running trouble / NAD / PAD sums used by snapshots */
   int device;        /* CUDA device ordinal the handle's memory and kernels live on */
   int kernel_path;   /* FVH_PATH_*: which kernel family runs the stage */
+  int dmr_split;     /* FVH_BC_DMR_Y0: first x index (ghosts negative) whose cell centre is >= 1/6 */
 } fvh_config;
 
 /* kernel families (identical results in FP64) */
@@ -166,7 +171,8 @@ int fvh_primitives(fvh_handle* h, const double* u, double* w, int fv_average, vo
  * holds until exit. cfg is checked as by fvh_create; grids needing more than
  * fvh_primitives_noalloc_max_doubles() doubles per buffer
  * (nvars * prod(n_a + 4 ceil(p_a/2)) over the active axes) are refused with
- * FVH_ERR_CONFIG. The first call on a device resolves the array's address
+ * FVH_ERR_CONFIG, and so are Dirichlet and FVH_BC_DMR_Y0 sides, whose
+ * ghost values live in a handle. The first call on a device resolves the array's address
  * (make it before any stream capture). All calls share the array: calls whose
  * work overlaps on the GPU race. Errors: fvh_primitives_noalloc_error(). */
 int fvh_primitives_noalloc(const fvh_config* cfg, const double* u, double* w, int fv_average, void* stream);
@@ -334,7 +340,8 @@ int fvh_pred_flags(fvh_handle* h, uint8_t* flags, void* stream);
  * reaches it, exactly as EulerSolver.ssprk3(t_end) does (fvhoe/ode.py:11-22,
  * 94-112); an FP64 member equals the same problem run alone, bit for bit.
  * cfg: the shared settings (cfg.n and cfg.h[0..1] are ignored; x and y must
- * be active, five variables, equal p in 1..8 on x and y, no convex weights).
+ * be active, five variables, equal p in 1..8 on x and y, no convex weights,
+ * no Dirichlet or FVH_BC_DMR_Y0 sides).
  * ------------------------------------------------------------------------ */
 typedef struct fvh_ensemble fvh_ensemble;
 

@@ -296,13 +296,41 @@ def _dirichlet_slab(cfg, axis: int, side: int, g: Sequence[int]) -> np.ndarray:
     return np.ones((cfg.nvars,) + X.shape) * np.asarray(value).reshape(-1, 1, 1, 1)
 
 
+DMR_Y0 = "special-case-double-mach-reflection-y=0"
+
+
+def _fill_axis(u: np.ndarray, g: int, axis: int, low: str, high: str) -> np.ndarray:
+    """u padded by g ghost cells of the given kinds along one spatial axis."""
+    src, flip = _ghost_source(u.shape[axis + 1], g, low, high)
+    out = np.take(u, src, axis=axis + 1)
+    if flip.any():
+        sel = [slice(None)] * 4
+        sel[0] = 1 + axis
+        sel[axis + 1] = flip
+        out[tuple(sel)] *= -1.0
+    return out
+
+
+def _dmr_free_columns(cfg, g: Sequence[int]) -> np.ndarray:
+    """Mask over the n_x + 2 g_x padded x columns: True where the low-y slab's
+    x centre (built slab_buffer_size deep, trimmed to g_x ghosts) is below 1/6
+    (fvhoe/boundary_conditions.py:375-377)."""
+    buffer = tuple(cfg.slab_buffer_size if act else 0 for act in cfg.active)
+    X = _slab_meshgen(cfg.n, cfg.domain, buffer)["yl"][0][:, 0, 0]
+    excess = buffer[0] - g[0]
+    X = X[excess:X.size - excess]
+    return X < 1 / 6
+
+
 def pad_with_ghosts(u: np.ndarray, g: Sequence[int], bc, cfg=None) -> np.ndarray:
     """Pad (nvars, nx, ny, nz) by g[a] ghost cells per spatial axis.
 
     periodic copies the opposite interior, outflow mirrors, reflective mirrors
     and negates the normal momentum, free repeats the edge cell
     (fvhoe/boundary_conditions.py:60-151), "dirichlet" and "ic" sides take
-    the values of cfg (:18-55); axes are filled x, then y, then z, each slab
+    the values of cfg (:18-55), the double-Mach-reflection wall on the low y
+    side is free or reflective by column (:374-395); axes are filled x, then
+    y, then z, each slab
     spanning the ghost layers of the axes filled before it, so corner ghosts
     take the last axis' treatment of the earlier axes' values (:324-400).
     """
@@ -314,13 +342,16 @@ def pad_with_ghosts(u: np.ndarray, g: Sequence[int], bc, cfg=None) -> np.ndarray
         dirichlet = [k in ("dirichlet", "ic") for k in kinds]
         mapped = [k if not d else "free" for k, d in zip(kinds, dirichlet)]
         n_a = out.shape[axis + 1]
-        src, flip = _ghost_source(n_a, g[axis], *mapped)
-        out = np.take(out, src, axis=axis + 1)
-        if flip.any():
-            sel = [slice(None)] * 4
-            sel[0] = 1 + axis
-            sel[axis + 1] = flip
-            out[tuple(sel)] *= -1.0
+        if kinds[0] == DMR_Y0:
+            # the double-Mach-reflection wall: both fills, chosen per x column
+            # by the low-y slab's x centre (fvhoe/boundary_conditions.py:374-395)
+            if axis != 1:
+                raise ValueError(f"'{DMR_Y0}' is defined on the low y side only")
+            free = _fill_axis(out, g[axis], axis, "free", mapped[1])
+            refl = _fill_axis(out, g[axis], axis, "reflective", mapped[1])
+            out = np.where(_dmr_free_columns(cfg, g)[None, :, None, None], free, refl)
+        else:
+            out = _fill_axis(out, g[axis], axis, *mapped)
         for side in range(2):
             if not dirichlet[side]:
                 continue

@@ -54,14 +54,32 @@ def box_z_high(x, y, z, t):
     return _conserved(rho, 0 * x, 0.05 + 0 * x, -0.3 + 0.2 * t + 0 * x, 1.0 + 0 * x)
 
 
+def dmr_inflow():
+    """The shocked gas of the double Mach reflection entering from the low x side."""
+    return _conserved(8.0, 7.145, -8.25 / 2, 0.0, 116.5).reshape(5)
+
+
+def dmr_top(x, y, z, t):
+    """The high y side of the double Mach reflection: shocked gas left of the
+    Mach-10 shock, inclined at 60 degrees and moving at 10 / sin(60 deg)
+    along x (Woodward and Colella's set-up), gas at rest right of it."""
+    theta = np.pi / 3
+    front = 10 * t / np.sin(theta) + 1 / 6 + y / np.tan(theta)
+    post = x < front
+    return _conserved(np.where(post, 8.0, GAMMA), np.where(post, 7.145, 0.0), np.where(post, -8.25 / 2, 0.0),
+                      0 * x, np.where(post, 116.5, 1.0))
+
+
 VALUES = {
     "inflow_state": inflow_state,
     "wall_y_low": wall_y_low,
     "wall_y_high": wall_y_high,
     "box_x_low": box_x_low,
     "box_z_high": box_z_high,
+    "dmr_inflow": dmr_inflow,
+    "dmr_top": dmr_top,
 }
-ARRAYS = {"inflow_state"}
+ARRAYS = {"inflow_state", "dmr_inflow"}
 
 
 def resolve(name):

@@ -37,14 +37,14 @@ def test_config_struct_layout_matches_header(tmp_path):
     src = tmp_path / "size.c"
     src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "fvh.h"\n'
                    'int main(){printf("%zu %zu %zu %zu %zu %d %d %d\\n", sizeof(fvh_config),'
-                   ' offsetof(fvh_config, device), offsetof(fvh_config, pad_hi), sizeof(fvh_stats),'
+                   ' offsetof(fvh_config, dmr_split), offsetof(fvh_config, pad_hi), sizeof(fvh_stats),'
                    ' sizeof(fvh_pred_stats), FVH_KK_COUNT, FVH_MLP_FEATURES, FVH_MLP_ROW);return 0;}\n')
     exe = tmp_path / "size"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()
-    size, dev, pad_hi, stats, pstats, kinds, feats, row = map(int, out)
+    size, split, pad_hi, stats, pstats, kinds, feats, row = map(int, out)
     assert size == ctypes.sizeof(_capi.FvhConfig)
-    assert dev == _capi.FvhConfig.device.offset
+    assert split == _capi.FvhConfig.dmr_split.offset
     assert pad_hi == _capi.FvhConfig.pad_hi.offset
     assert stats == ctypes.sizeof(_capi.FvhStats)
     assert pstats == ctypes.sizeof(_capi.FvhPredStats)
@@ -109,6 +109,9 @@ def test_default_config_matches_reference_defaults():
         (dict(nvars=4), "nvars must be in [5, 16]"),
         (dict(riemann=7), "unknown Riemann solver"),
         (dict(bc=((1, 0), (0, 0), (0, 0))), "periodic high boundary"),
+        (dict(bc=((5, 1), (0, 0), (0, 0))), "low y side only"),
+        (dict(bc=((1, 1), (1, 5), (0, 0)), n=(64, 32, 1), p=(3, 3, 0)), "low y side only"),
+        (dict(bc=((1, 1), (6, 1), (0, 0)), n=(64, 32, 1), p=(3, 3, 0)), "unsupported boundary kind"),
         (dict(n=(1, 1, 1), p=(0, 0, 0)), "no active axis"),
         (dict(a_posteriori=1, convex=1, n=(32, 32, 32), p=(1, 1, 1)), "3D convex"),
         (dict(pad_var=7), "pad_var"),
@@ -164,8 +167,12 @@ def test_boundary_condition_parsing_and_refusals():
     bc = BoundaryCondition(x=("reflective", "outflow"), y="free")
     assert bc.x == ("reflective", "outflow") and bc.y == ("free", "free") and bc.z == ("periodic", "periodic")
     assert bc.kinds((True, True, False))[0] == ("reflective", "outflow")
-    with pytest.raises(NotImplementedError):
-        BoundaryCondition(y="special-case-double-mach-reflection-y=0").kinds((True, True, False))
+    # the double-Mach-reflection wall exists on the low y side only
+    dmr = "special-case-double-mach-reflection-y=0"
+    assert BoundaryCondition(y=(dmr, "outflow")).kinds((True, True, False))[1] == (dmr, "outflow")
+    for bad in (dict(y=dmr), dict(y=("outflow", dmr)), dict(x=(dmr, "outflow"))):
+        with pytest.raises(ValueError):
+            BoundaryCondition(**bad).kinds((True, True, False))
     # Dirichlet sides need a callable or an array of values (the reference raises when it applies them)
     with pytest.raises(ValueError):
         BoundaryCondition(x="dirichlet").kinds((True, False, False))
@@ -265,6 +272,7 @@ def test_snapshot_list_settles_before_reads_and_pickles_as_a_list():
     ("ShockTube", dict(dims="xy", center=(0.5, 0.5), radius=0.3), True),
     ("ShockTube", dict(mode="cube", x_cube=(0.2, 0.6), y_cube=(0.3, 0.9)), True),
     ("FourQuadrant2D", dict(seed=7), True),
+    ("DoubleMachReflection2D", dict(), True),
     ("SedovBlast", dict(mode="corner", dims="xy"), True),
     ("Sinus", dict(dims="xy"), False),
     ("ShuOsher1D", dict(), False),
@@ -295,3 +303,40 @@ def test_initial_conditions_evaluate_on_torch_tensors(name, kw, exact):
         assert np.array_equal(dev.numpy(), host)
     else:
         assert np.allclose(dev.numpy(), host, rtol=1e-14, atol=1e-15)
+
+
+def test_dmr_split_matches_oracle_columns():
+    """The split the solver hands to the library selects the same free columns
+    as the oracle's restatement of the reference's X < 1/6 mask."""
+    from types import SimpleNamespace
+
+    from fvhoe_b200.boundary_conditions import dmr_split
+    from oracle import fvh_oracle as O
+
+    for n, domain, g in (((48, 12, 1), ((0, 4), (0, 1), (0, 1)), (8, 8, 0)),
+                         ((40, 20, 1), ((0, 4), (0, 1), (0, 1)), (11, 11, 0)),
+                         ((30, 10, 1), ((-1, 2), (0, 1), (0, 1)), (5, 5, 0)),
+                         ((16, 16, 1), ((0.2, 1.0), (0, 1), (0, 1)), (6, 6, 0)),
+                         ((12, 8, 1), ((-3, -1), (0, 1), (0, 1)), (4, 4, 0))):
+        buffer = (30, 30, 0)
+        cfg = SimpleNamespace(n=n, domain=domain, slab_buffer_size=30, active=(True, True, False))
+        cols = O._dmr_free_columns(cfg, g)
+        split = dmr_split(n, *domain, buffer)
+        assert np.array_equal(cols, np.arange(-g[0], n[0] + g[0]) < split)
+
+
+@pytest.mark.parametrize("fixture", ["rhs_dmr_p3.npz", "rhs_dmr_p7_llf.npz"])
+def test_double_mach_reflection_ic_matches_reference_state(fixture):
+    """DoubleMachReflection2D gives the reference's initial conserved state
+    (the fixture's u0, made by fvhoe's own DoubleMachReflection2D), bit for bit."""
+    from fvhoe_b200.fv import fv_uniform_meshgen
+    from fvhoe_b200.hydro import HydroState
+    from fvhoe_b200.initial_conditions import DoubleMachReflection2D
+    from fvhoe_b200.solver import _ic_functions
+    from tests.fixtures import load
+
+    c, d = load(os.path.join(ROOT, "tests", "golden", fixture))
+    _, _, u0_fv = _ic_functions(DoubleMachReflection2D(), HydroState(), None, False, False, c["gamma"],
+                                tuple(c["h"]), tuple(c["p"]))
+    X, Y, Z = fv_uniform_meshgen(tuple(c["n"]), *[tuple(r) for r in c["domain"]])
+    assert np.array_equal(u0_fv(X, Y, Z), d["u0"])
