@@ -153,7 +153,11 @@ int fvh_rhs(fvh_handle* h, const double* u, double* dudt, double* dt_out, void* 
  * stage's dt is shortened to target - t when has_target is set and the target
  * is closer (fvhoe/ode.py:11-22). Replaces ODE.take_step with the stepper of
  * ODE.euler/ssprk2/ssprk3/rk4 (fvhoe/ode.py:183-193, 245-298).
- * dt_out: host pointer or NULL (when given, the stream is synchronised). */
+ * dt_out: host pointer or NULL (when given, the stream is synchronised). With
+ * dt_out = NULL the call makes no host synchronisation and can be captured in
+ * a CUDA graph after one uncaptured call of the same handle; each replay
+ * computes its own dt on the device and reuses the captured t, target and
+ * trouble-log mode, so capture steps without a target (or with a fixed one). */
 int fvh_step(fvh_handle* h, double* u, int integrator, double t, int has_target, double target, double* dt_out,
              void* stream);
 

@@ -238,3 +238,41 @@ def test_double_mach_reflection_fused_equals_generic(p):
     rel = np.mean(np.abs(r - a[0])) / np.mean(np.abs(a[0]))
     print(f"dmr p={p} fp32 relative L1 {rel:.3e}")
     assert rel < 1e-3, rel
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_step_captured_in_a_cuda_graph_equals_eager_steps(precision):
+    """fvh_step with dt_out = NULL makes no host synchronisation, so a whole
+    SSP-RK3 step (its fifteen fused launches and the scalar resets) can be
+    captured in a CUDA graph; replaying it gives the eagerly stepped states bit
+    for bit (dt is computed and used on the device every replay)."""
+    import ctypes
+
+    import torch
+
+    from fvhoe_b200 import EulerSolver, KelvinHelmholtzNoise2D, _capi
+
+    kw = dict(w0=KelvinHelmholtzNoise2D(n=(128, 96), seed=4), nx=128, ny=96, px=5, py=5, gamma=1.4,
+              riemann_solver="hllc", a_posteriori_slope_limiting=True, NAD=1e-5, progress_bar=False,
+              precision=precision)
+    eager, graphed = EulerSolver(**kw), EulerSolver(**kw)
+    lib, ssprk3 = _capi.lib, _capi.INTEGRATOR["ssprk3"]
+
+    def step(s, stream):
+        u = ctypes.c_void_p(s.am("u").data_ptr())
+        _capi.check(lib.fvh_step(s._handle, u, ssprk3, 0.0, 0, 0.0, None, ctypes.c_void_p(stream)), s._handle)
+
+    cur = torch.cuda.current_stream().cuda_stream
+    for _ in range(4):
+        step(eager, cur)
+    step(graphed, cur)  # warm-up outside the capture (module loading, shared-memory attributes)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    with torch.cuda.graph(g, stream=side):
+        step(graphed, torch.cuda.current_stream().cuda_stream)
+    for _ in range(3):
+        g.replay()
+    torch.cuda.synchronize()
+    assert np.array_equal(graphed.am.get_numpy("u"), eager.am.get_numpy("u"))
+    del g
