@@ -44,7 +44,7 @@ def parse():
                     help="common time at which the L1 density error against fp64 is taken")
     ap.add_argument("--n", type=int, default=2048, help="cells per side")
     ap.add_argument("--p", type=int, default=5)
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-sample", type=int, default=512, help="side of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain fp64 comparison (profiling runs)")
@@ -615,14 +615,25 @@ def run_ours(args):
                 "stage_model": {"bytes_per_cell_update": 120,
                                 "achieved_gb_s": 120 * value / world * 1e6 / 1e9}}
 
-    # end to end through the C ABI with host buffers: per step, copy the state in from
-    # pinned host memory, run the step with its dt read-back, copy the state out
+    # end to end through the C ABI with the state in pinned host memory: every step
+    # copies the whole state in, steps it (dt read back) and copies it out.
+    # fvh_step_host pipelines the copies in chunks (a step's copy-out overlaps the
+    # next step's copy-in); the serial form (copy in, step, copy out, wait) is
+    # timed too for comparison.
     host = torch.empty(u.shape, dtype=torch.float64, pin_memory=True)
     host.copy_(u)
     torch.cuda.synchronize()
     nbytes = u.numel() * 8
     dt = ctypes.c_double()
     ssprk3 = _capi.INTEGRATOR["ssprk3"]
+    hptr = ctypes.c_void_p(host.data_ptr())
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        _capi.check(lib.fvh_set_log_mode(h, 1), h)
+        _capi.check(lib.fvh_set_log_divisor(h, 3.0), h)
+        _capi.check(lib.fvh_step_host(h, hptr, ssprk3, 0.0, 0, 0.0, ctypes.byref(dt), sp), h)
+    _capi.check(lib.fvh_host_sync(h), h)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
         u.copy_(host, non_blocking=True)
@@ -631,11 +642,12 @@ def run_ours(args):
         _capi.check(lib.fvh_step(h, uptr, ssprk3, 0.0, 0, 0.0, ctypes.byref(dt), sp), h)
         host.copy_(u, non_blocking=True)
         stream.synchronize()
-    e2e_s = time.perf_counter() - t0
-    e2e_s = max_over_ranks(e2e_s, dist)
+    serial_s = max_over_ranks(time.perf_counter() - t0, dist)
     e2e = {"value": world * 3 * cells * args.e2e_steps / e2e_s / 1e6, "unit": UNIT,
            "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": args.e2e_steps,
-           "path": "fvh_step through the C ABI; state copied from/to pinned host memory every step"}
+           "path": "fvh_step_host through the C ABI: state in pinned host memory, copied in and out every "
+                   "step in 16 chunks on two copy streams",
+           "serial_value": world * 3 * cells * args.e2e_steps / serial_s / 1e6}
 
     stats = chosen.stats()
     if rank == 0:

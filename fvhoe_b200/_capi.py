@@ -36,6 +36,8 @@ EXPORTS = (
     "fvh_scratch_bytes",
     "fvh_rhs",
     "fvh_step",
+    "fvh_step_host",
+    "fvh_host_sync",
     "fvh_primitives",
     "fvh_trouble_flags",
     "fvh_trouble_log",
@@ -168,6 +170,8 @@ def _load():
     lib.fvh_scratch_bytes.restype = ctypes.c_size_t
     lib.fvh_rhs.argtypes = [vp, vp, vp, dp, vp]
     lib.fvh_step.argtypes = [vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, dp, vp]
+    lib.fvh_step_host.argtypes = [vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, dp, vp]
+    lib.fvh_host_sync.argtypes = [vp]
     lib.fvh_primitives.argtypes = [vp, vp, vp, ctypes.c_int, vp]
     lib.fvh_trouble_flags.argtypes = [vp, vp, vp]
     lib.fvh_trouble_log.argtypes = [vp, ctypes.c_double, vp, vp, vp, vp]
@@ -232,7 +236,8 @@ def _load():
                  "fvh_ensemble_status", "fvh_ensemble_configure", "fvh_ensemble_variant_info",
                  "fvh_ensemble_autotune", "fvh_ensemble_graph_info"):
         getattr(lib, name).restype = ctypes.c_int
-    for name in ("fvh_create", "fvh_destroy", "fvh_rhs", "fvh_step", "fvh_primitives", "fvh_trouble_flags",
+    for name in ("fvh_create", "fvh_destroy", "fvh_rhs", "fvh_step", "fvh_step_host", "fvh_host_sync",
+                 "fvh_primitives", "fvh_trouble_flags",
                  "fvh_trouble_log", "fvh_set_log_mode", "fvh_get_stats", "fvh_profile_enable", "fvh_profile_read",
                  "fvh_mlp_create", "fvh_mlp_destroy", "fvh_mlp_get_params", "fvh_mlp_set_params", "fvh_mlp_features",
                  "fvh_mlp_train_step", "fvh_mlp_gradients", "fvh_mlp_logits", "fvh_set_predictor",

@@ -276,6 +276,15 @@ void release(fvh_handle* h) {
   cudaSetDevice(h->cfg.device);
   delete h->prof;
   h->prof = nullptr;
+  if (h->copy_out) cudaStreamSynchronize(h->copy_out);
+  if (h->copy_in) cudaStreamSynchronize(h->copy_in);
+  for (cudaEvent_t& e : h->out_done)
+    if (e) cudaEventDestroy(e);
+  if (h->in_done) cudaEventDestroy(h->in_done);
+  if (h->step_done) cudaEventDestroy(h->step_done);
+  if (h->copy_in) cudaStreamDestroy(h->copy_in);
+  if (h->copy_out) cudaStreamDestroy(h->copy_out);
+  if (h->host_state) cudaFree(h->host_state);
   void* ptrs[] = {h->bufA, h->bufB, h->W,        h->Ws,       h->Us,       h->F[0],     h->F[1],
                   h->F[2], h->trouble, h->logs[0], h->logs[1], h->logs[2], h->acc,      h->S[0],
                   h->S[1], h->theta[0], h->theta[1], h->theta[2], h->conv, h->sc, h->pred, h->slabs_dev,
@@ -395,6 +404,21 @@ int read_dt(fvh_handle* h, cudaStream_t s, double* dt_out) {
     return FVH_ERR_CUDA;
   }
   *dt_out = host.dt_step;
+  return FVH_OK;
+}
+
+// Device copy, copy streams and events of fvh_step_host, made on its first call.
+int host_path_init(fvh_handle* h) {
+  if (h->host_state) return FVH_OK;
+  const size_t bytes = (size_t)h->nv * h->n[0] * h->n[1] * h->n[2] * sizeof(double);
+  if (int st = alloc(h, (void**)&h->host_state, bytes)) return st;
+  cudaError_t e = cudaStreamCreateWithFlags(&h->copy_in, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->copy_out, cudaStreamNonBlocking);
+  for (int j = 0; j < fvh_handle::kHostChunks && e == cudaSuccess; ++j)
+    e = cudaEventCreateWithFlags(&h->out_done[j], cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->in_done, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->step_done, cudaEventDisableTiming);
+  if (e != cudaSuccess) return fail(h, FVH_ERR_CUDA, std::string("host path set-up: ") + cudaGetErrorString(e));
   return FVH_OK;
 }
 
@@ -540,6 +564,58 @@ int fvh_step(fvh_handle* h, double* u, int integrator, double t, int has_target,
   }
   h->log_divisor = 0.0;
   return read_dt(h, s, dt_out);
+}
+
+int fvh_step_host(fvh_handle* h, double* u_host, int integrator, double t, int has_target, double target,
+                  double* dt_out, void* stream) {
+  if (!h) return FVH_ERR_ARG;
+  if (!u_host) return fail(h, FVH_ERR_ARG, "null array");
+  if (int st0 = use_device(h)) return st0;
+  if (int st0 = host_path_init(h)) return st0;
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t count = (size_t)h->nv * h->n[0] * h->n[1] * h->n[2];
+  constexpr int NC = fvh_handle::kHostChunks;
+  auto chunk = [&](int j, size_t& off, size_t& len) {
+    off = count * j / NC;
+    len = count * (j + 1) / NC - off;
+  };
+  cudaError_t e = cudaSuccess;
+  // copy-in: chunk j waits only for chunk j of the previous call's copy-out
+  for (int j = 0; j < NC && e == cudaSuccess; ++j) {
+    size_t off, len;
+    chunk(j, off, len);
+    if (h->out_pending) e = cudaStreamWaitEvent(h->copy_in, h->out_done[j], 0);
+    if (e == cudaSuccess && len)
+      e = cudaMemcpyAsync(h->host_state + off, u_host + off, len * sizeof(double), cudaMemcpyHostToDevice,
+                          h->copy_in);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(h->in_done, h->copy_in);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s, h->in_done, 0);
+  if (e != cudaSuccess) return fail(h, FVH_ERR_CUDA, std::string("copy-in: ") + cudaGetErrorString(e));
+  if (int st = fvh_step(h, h->host_state, integrator, t, has_target, target, nullptr, stream)) return st;
+  // copy-out on its own stream, chunk by chunk, each chunk's completion recorded
+  e = cudaEventRecord(h->step_done, s);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(h->copy_out, h->step_done, 0);
+  for (int j = 0; j < NC && e == cudaSuccess; ++j) {
+    size_t off, len;
+    chunk(j, off, len);
+    if (len)
+      e = cudaMemcpyAsync(u_host + off, h->host_state + off, len * sizeof(double), cudaMemcpyDeviceToHost,
+                          h->copy_out);
+    if (e == cudaSuccess) e = cudaEventRecord(h->out_done[j], h->copy_out);
+  }
+  if (e != cudaSuccess) return fail(h, FVH_ERR_CUDA, std::string("copy-out: ") + cudaGetErrorString(e));
+  h->out_pending = true;
+  return read_dt(h, s, dt_out);
+}
+
+int fvh_host_sync(fvh_handle* h) {
+  if (!h) return FVH_ERR_ARG;
+  if (!h->copy_out) return FVH_OK;
+  if (int st0 = use_device(h)) return st0;
+  const cudaError_t e = cudaStreamSynchronize(h->copy_out);
+  if (e != cudaSuccess) return fail(h, FVH_ERR_CUDA, std::string("copy-out: ") + cudaGetErrorString(e));
+  return FVH_OK;
 }
 
 int fvh_primitives(fvh_handle* h, const double* u, double* w, int fv_average, void* stream) {

@@ -54,6 +54,15 @@ struct fvh_handle {
   long long pred_stage = 0;       // fused stages run since the predictor was attached
   bool last_stage_fused = false;  // the last stage ran the fused 2D kernels
 
+  // host-resident state (fvh_step_host): device copy, two copy streams and
+  // the per-chunk events that let one call's copy-in follow the previous
+  // call's copy-out chunk by chunk
+  static constexpr int kHostChunks = 16;
+  double* host_state = nullptr;   // device copy of the host state
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  cudaEvent_t out_done[kHostChunks] = {};  // copy-out of chunk j finished
+  cudaEvent_t in_done = nullptr, step_done = nullptr;
+  bool out_pending = false;       // out_done events recorded by an earlier call
   int log_mode_next = 1;          // log mode of the next stage
   double log_divisor = 0.0;       // divisor applied by the next step's last stage (one-shot)
   fvh::Profiler* prof = nullptr;  // per-launch timing, when enabled

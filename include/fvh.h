@@ -161,6 +161,23 @@ int fvh_rhs(fvh_handle* h, const double* u, double* dudt, double* dt_out, void* 
 int fvh_step(fvh_handle* h, double* u, int integrator, double t, int has_target, double target, double* dt_out,
              void* stream);
 
+/* fvh_step for a state held in page-locked host memory (cudaHostAlloc or
+ * cudaHostRegister), as the reference holds u in host NumPy arrays: the call
+ * copies u_host in, steps it and copies the result back to u_host, all queued
+ * on the handle's two copy streams and the caller's stream. Both copies run in
+ * 16 contiguous chunks, and chunk j of a call's copy-in waits only for chunk j
+ * of the previous call's copy-out, so on a full-duplex link one step's
+ * copy-out overlaps the next step's copy-in. The call returns once the work is
+ * queued (after the step when dt_out is given, which synchronises the caller's
+ * stream only); u_host must not be read or written until fvh_host_sync(h)
+ * returns. The device copy (nvars * nx * ny * nz doubles) and the streams are
+ * made on the first call and counted by fvh_scratch_bytes. No counterpart in
+ * the reference, whose state never leaves the host. */
+int fvh_step_host(fvh_handle* h, double* u_host, int integrator, double t, int has_target, double target,
+                  double* dt_out, void* stream);
+/* Waits for the copy-out of the last fvh_step_host call. */
+int fvh_host_sync(fvh_handle* h);
+
 /* Finite-volume primitive averages (fv_average = 1) or cell-centre primitives
  * (fv_average = 0) of u over the interior, written to w (same shape).
  * Replaces interpolate_primitives_from_conservatives with gw = 0

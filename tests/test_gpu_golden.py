@@ -276,3 +276,35 @@ def test_step_captured_in_a_cuda_graph_equals_eager_steps(precision):
     torch.cuda.synchronize()
     assert np.array_equal(graphed.am.get_numpy("u"), eager.am.get_numpy("u"))
     del g
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_host_state_steps_equal_device_steps(precision):
+    """fvh_step_host (state in page-locked host memory, chunked copies on two
+    copy streams, one call's copy-in following the previous call's copy-out)
+    gives, after every step, the state fvh_step gives on the device."""
+    import ctypes
+
+    import torch
+
+    from fvhoe_b200 import EulerSolver, KelvinHelmholtzNoise2D, _capi
+
+    kw = dict(w0=KelvinHelmholtzNoise2D(n=(136, 100), seed=6), nx=136, ny=100, px=5, py=5, gamma=1.4,
+              riemann_solver="hllc", a_posteriori_slope_limiting=True, NAD=1e-5, progress_bar=False,
+              precision=precision)
+    dev, host_side = EulerSolver(**kw), EulerSolver(**kw)
+    lib, ssprk3 = _capi.lib, _capi.INTEGRATOR["ssprk3"]
+    host = torch.empty(host_side.am("u").shape, dtype=torch.float64, pin_memory=True)
+    host.copy_(host_side.am("u"))
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    dt_dev, dt_host = ctypes.c_double(), ctypes.c_double()
+    u_dev = ctypes.c_void_p(dev.am("u").data_ptr())
+    for k in range(5):
+        _capi.check(lib.fvh_step(dev._handle, u_dev, ssprk3, 0.0, 0, 0.0, ctypes.byref(dt_dev), stream), dev._handle)
+        _capi.check(lib.fvh_step_host(host_side._handle, ctypes.c_void_p(host.data_ptr()), ssprk3, 0.0, 0, 0.0,
+                                      ctypes.byref(dt_host), stream), host_side._handle)
+        assert dt_host.value == dt_dev.value
+        if k in (0, 4):
+            _capi.check(lib.fvh_host_sync(host_side._handle), host_side._handle)
+            assert np.array_equal(host.numpy(), dev.am.get_numpy("u"))
+    assert lib.fvh_host_sync(None) == _capi.ERR_ARG
