@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--pred-accuracy-time", type=float, default=0.002)
     ap.add_argument("--pred-every", type=int, default=3,
                     help="stages between predictions of the second learned form (3: once per SSP-RK3 step)")
+    ap.add_argument("--no-sedov", action="store_true", help="skip the 3D Sedov leg")
+    ap.add_argument("--sedov-n", type=int, default=256, help="cells per side of the 3D Sedov leg")
+    ap.add_argument("--sedov-steps", type=int, default=5, help="timed steps of each form in the Sedov leg")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
     ap.add_argument("--ens-members", type=int, default=256)
     ap.add_argument("--ens-steps", type=int, default=10, help="timed ensemble steps")
@@ -440,6 +443,51 @@ def ensemble_members(count, seed=2024, side=None):
 ENSEMBLE_KW = dict(gamma=1.4, riemann_solver="hllc", CFL=0.8, a_posteriori_slope_limiting=True, NAD=1e-5)
 
 
+def sedov_leg(args, stream, sp):
+    """The 3D Sedov configuration on the generic N-D kernels: sedov_n^3 cells of
+    [0,1]^3, p = 3, LLF, SSP-RK3, CFL 0.5, reflective at the x = 0, y = 0, z = 0
+    faces and outflow elsewhere, a-posteriori MUSCL with NAD and PAD, the blast
+    energy in the corner cell. Timed steps (CUDA events, state on the device) of
+    the plain FP64 path and of the FP32 form, and the L1 density difference
+    between the two after the same steps."""
+    import ctypes
+
+    import torch
+
+    from fvhoe_b200 import BoundaryCondition, EulerSolver, SedovBlast, _capi
+
+    lib = _capi.lib
+    n = args.sedov_n
+    cells = n ** 3
+    bc = BoundaryCondition(x=("reflective", "outflow"), y=("reflective", "outflow"), z=("reflective", "outflow"))
+
+    def make(precision):
+        return EulerSolver(w0=SedovBlast(dims="xyz"), conservative_ic=True, fv_ic=True, nx=n, ny=n, nz=n, px=3,
+                           py=3, pz=3, gamma=1.4, riemann_solver="llf", CFL=0.5, bc=bc,
+                           a_posteriori_slope_limiting=True, progress_bar=False, precision=precision,
+                           ic_on_device=True)
+
+    out = {"config": f"3D Sedov {n}^3, p=3, LLF, SSP-RK3, CFL 0.5, reflective origin faces, outflow elsewhere, "
+                     "a-posteriori MUSCL with NAD + PAD; generic N-D kernels", "cells": cells}
+    rho = {}
+    for precision in ("fp64", "fp32"):
+        s = make(precision)
+        up = ctypes.c_void_p(s.am("u").data_ptr())
+        _time_steps(lib, _capi, s._handle, up, sp, stream, args.warmup)
+        ms, _ = _time_steps(lib, _capi, s._handle, up, sp, stream, args.sedov_steps)
+        out[precision] = {"mcell_updates_per_s": 3 * cells * args.sedov_steps / (ms / 1e3) / 1e6,
+                          "ms_per_step": ms / args.sedov_steps, "scratch_bytes": lib.fvh_scratch_bytes(s._handle),
+                          "nonfinite": s.stats()["nonfinite"]}
+        rho[precision] = s.am("u")[0].double().clone()
+        del s
+        torch.cuda.empty_cache()
+    out["speedup_fp32_vs_fp64"] = out["fp32"]["mcell_updates_per_s"] / out["fp64"]["mcell_updates_per_s"]
+    steps = args.warmup + args.sedov_steps
+    out["l1_density_difference_fp32_vs_fp64"] = (rho["fp32"] - rho["fp64"]).abs().mean().item()
+    out["note"] = f"both forms advanced {steps} steps from the same state, each with its own CFL dt"
+    return out
+
+
 def ensemble_leg(args, stream, members=None, label=None):
     """256 independent four-quadrant problems (p=3, HLLC, SSP-RK3, CFL 0.8,
     outflow, a-posteriori NAD 1e-5 + PAD + SED, FP32 with FP64 stage
@@ -671,6 +719,12 @@ def run_ours(args):
                 line["learned_predictor"] = predictor_leg(args, stream, sp)
             except Exception as exc:  # the headline line is printed whatever this leg does
                 line["learned_predictor"] = {"error": f"{type(exc).__name__}: {exc}"}
+        if world == 1 and not args.no_sedov:
+            torch.cuda.empty_cache()
+            try:
+                line["sedov_3d"] = sedov_leg(args, stream, sp)
+            except Exception as exc:
+                line["sedov_3d"] = {"error": f"{type(exc).__name__}: {exc}"}
         if world == 1 and not args.no_ensemble:
             torch.cuda.empty_cache()
             try:
