@@ -478,6 +478,18 @@ def sedov_leg(args, stream, sp):
         out[precision] = {"mcell_updates_per_s": 3 * cells * args.sedov_steps / (ms / 1e3) / 1e6,
                           "ms_per_step": ms / args.sedov_steps, "scratch_bytes": lib.fvh_scratch_bytes(s._handle),
                           "nonfinite": s.stats()["nonfinite"]}
+        # per-kind device time of one more step (CUDA events around each launch)
+        h = s._handle
+        _capi.check(lib.fvh_profile_enable(h, 1), h)
+        _time_steps(lib, _capi, h, up, sp, stream, 1)
+        K = len(_capi.KERNEL_KINDS)
+        pms = (ctypes.c_double * K)()
+        plaunch = (ctypes.c_uint64 * K)()
+        _capi.check(lib.fvh_profile_read(h, pms, None, plaunch, sp), h)
+        _capi.check(lib.fvh_profile_enable(h, 0), h)
+        out[precision]["kernels_ms_per_step"] = {nm: round(pms[i], 3) for i, nm in enumerate(_capi.KERNEL_KINDS)
+                                                 if plaunch[i]}
+        out[precision]["launches_per_step"] = int(sum(plaunch))
         rho[precision] = s.am("u")[0].double().clone()
         del s
         torch.cuda.empty_cache()
