@@ -222,6 +222,9 @@ def build_cases():
         domain=((0, 4), (0, 1), (0, 1)), riemann_solver="llf", **lim)
     add("steps", "dmr_p3", DoubleMachReflection2D(), (48, 12, 1), (3, 3, 0), steps=3, gamma=1.4, bc=dmr,
         domain=((0, 4), (0, 1), (0, 1)), riemann_solver="hllc", **lim)
+    # the wall in 3D (z periodic), where z ghosts are filled after it
+    add("rhs", "dmr3d_p2", DoubleMachReflection2D(), (24, 12, 8), (2, 2, 2), gamma=1.4, bc=dict(dmr, z="periodic"),
+        domain=((0, 2), (0, 1), (0, 0.5)), riemann_solver="hllc", **lim)
     return cases
 
 
