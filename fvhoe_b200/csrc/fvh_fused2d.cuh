@@ -897,8 +897,11 @@ __global__ void __launch_bounds__(256, 6)
 // (fvhoe/ode.py:245-298; the expressions of k_final, evaluated in the same
 // order) for integrator INTEG at stage STAGE. Every array the stage reads is
 // loaded for all five variables before the first store, so a cell's loads are
-// in flight together. Returns how many results are not finite.
-template <int INTEG, int STAGE>
+// in flight together. SO: SSP-RK3 in the Shu-Osher form instead of the
+// reference's k-sum form (the FP32 form: the same scheme, FP64 rounding apart,
+// reading the stage input in place of the k-sum and writing no k-sum).
+// Returns how many results are not finite.
+template <int INTEG, int STAGE, bool SO = false>
 __device__ __forceinline__ unsigned int rk_combine(const StageSpec& st, int o, int plane, double dt,
                                                    const double* k) {
   double a[5], b[5], res[5];
@@ -930,6 +933,27 @@ __device__ __forceinline__ unsigned int rk_combine(const StageSpec& st, int o, i
       } else {
         res[v] = 0.5 * a[v] + 0.5 * (b[v] + dt * k[v]);
         st.u[o + v * plane] = res[v];
+      }
+    }
+  } else if constexpr (INTEG == INT_SSPRK3 && SO) {
+    // u1 = u + dt k1; u2 = 3/4 u + 1/4 (u1 + dt k2); u3 = 1/3 u + 2/3 (u2 + dt k3)
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      a[v] = st.u[o + v * plane];
+      if constexpr (STAGE != 0) b[v] = st.stage_in[o + v * plane];
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const int ov = o + v * plane;
+      if constexpr (STAGE == 0) {
+        res[v] = a[v] + dt * k[v];
+        st.next[ov] = res[v];
+      } else if constexpr (STAGE == 1) {
+        res[v] = 0.75 * a[v] + 0.25 * (b[v] + dt * k[v]);
+        st.next[ov] = res[v];
+      } else {
+        res[v] = (1.0 / 3.0) * a[v] + (2.0 / 3.0) * (b[v] + dt * k[v]);
+        st.u[ov] = res[v];
       }
     }
   } else if constexpr (INTEG == INT_SSPRK3) {
@@ -985,6 +1009,7 @@ __device__ __forceinline__ unsigned int rk_combine(const StageSpec& st, int o, i
 }
 
 // rk_combine for the integrator and stage named at run time (the batched ensemble)
+template <bool SO>
 __device__ __forceinline__ unsigned int rk_combine_rt(const StageSpec& st, int o, int plane, double dt,
                                                       const double* k) {
   switch (st.integrator) {
@@ -994,9 +1019,9 @@ __device__ __forceinline__ unsigned int rk_combine_rt(const StageSpec& st, int o
       return st.stage == 0 ? rk_combine<INT_SSPRK2, 0>(st, o, plane, dt, k)
                            : rk_combine<INT_SSPRK2, 1>(st, o, plane, dt, k);
     case INT_SSPRK3:
-      if (st.stage == 0) return rk_combine<INT_SSPRK3, 0>(st, o, plane, dt, k);
-      if (st.stage == 1) return rk_combine<INT_SSPRK3, 1>(st, o, plane, dt, k);
-      return rk_combine<INT_SSPRK3, 2>(st, o, plane, dt, k);
+      if (st.stage == 0) return rk_combine<INT_SSPRK3, 0, SO>(st, o, plane, dt, k);
+      if (st.stage == 1) return rk_combine<INT_SSPRK3, 1, SO>(st, o, plane, dt, k);
+      return rk_combine<INT_SSPRK3, 2, SO>(st, o, plane, dt, k);
     default:
       if (st.stage == 0) return rk_combine<INT_RK4, 0>(st, o, plane, dt, k);
       if (st.stage == 1) return rk_combine<INT_RK4, 1>(st, o, plane, dt, k);
@@ -1102,9 +1127,9 @@ __device__ __forceinline__ void tile2_final(const double* __restrict__ stage_in,
       k[v] = (double)dc;
     }
     if constexpr (RKI >= 0) {
-      bad += rk_combine<RKI, RKS>(st, x * g.ny + y, plane, dt, k);
+      bad += rk_combine<RKI, RKS, sizeof(Tc) == 4>(st, x * g.ny + y, plane, dt, k);
     } else {
-      bad += rk_combine_rt(st, x * g.ny + y, plane, dt, k);
+      bad += rk_combine_rt<sizeof(Tc) == 4>(st, x * g.ny + y, plane, dt, k);
     }
   }
   block_count_add(bad, &sc->nonfinite);

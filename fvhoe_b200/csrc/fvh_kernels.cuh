@@ -899,7 +899,19 @@ __global__ void __launch_bounds__(256) k_final(Box box, View<double> state, Flux
           }
           break;
         case INT_SSPRK3:
-          if (st.stage == 0) {
+          if (sizeof(Tc) == 4) {
+            // FP32 form: the Shu-Osher stages (no k-sum), as the fused final pass
+            if (st.stage == 0) {
+              res = st.u[o] + dt * k;
+              st.next[o] = res;
+            } else if (st.stage == 1) {
+              res = 0.75 * st.u[o] + 0.25 * (st.stage_in[o] + dt * k);
+              st.next[o] = res;
+            } else {
+              res = (1.0 / 3.0) * st.u[o] + (2.0 / 3.0) * (st.stage_in[o] + dt * k);
+              st.u[o] = res;
+            }
+          } else if (st.stage == 0) {
             st.acc[o] = k;
             res = st.u[o] + dt * k;
             st.next[o] = res;

@@ -522,7 +522,8 @@ int run_stage_t(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     switch (c.spec.integrator) {
       case INT_EULER: arrays = 2; break;
       case INT_SSPRK2: arrays = c.spec.stage == 0 ? 2 : 3; break;
-      case INT_SSPRK3: arrays = c.spec.stage == 1 ? 4 : 3; break;
+      // FP32: the Shu-Osher stages read u (and the stage input) and write one array
+      case INT_SSPRK3: arrays = sizeof(Tc) == 4 ? (c.spec.stage == 0 ? 2 : 3) : (c.spec.stage == 1 ? 4 : 3); break;
       case INT_RK4: arrays = c.spec.stage == 0 ? 3 : (c.spec.stage == 3 ? 3 : 4); break;
       default: arrays = 1; break;
     }
@@ -707,7 +708,8 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     switch (c.spec.integrator) {
       case INT_EULER: arrays = 2; break;
       case INT_SSPRK2: arrays = c.spec.stage == 0 ? 2 : 3; break;
-      case INT_SSPRK3: arrays = c.spec.stage == 1 ? 4 : 3; break;
+      // FP32: the Shu-Osher stages read u (and the stage input) and write one array
+      case INT_SSPRK3: arrays = sizeof(Tc) == 4 ? (c.spec.stage == 0 ? 2 : 3) : (c.spec.stage == 1 ? 4 : 3); break;
       case INT_RK4: arrays = c.spec.stage == 0 ? 3 : (c.spec.stage == 3 ? 3 : 4); break;
       default: arrays = 1; break;
     }

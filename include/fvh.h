@@ -65,7 +65,8 @@ extern "C" {
 
 /* precision modes */
 #define FVH_PREC_FP64 0 /* every operation in float64, reference evaluation order, no FMA contraction */
-#define FVH_PREC_FP32 1 /* reconstruction, Riemann fluxes, detection in float32; float64 stage accumulation */
+#define FVH_PREC_FP32 1 /* reconstruction, Riemann fluxes, detection in float32; float64 stage accumulation
+                           (SSP-RK3 in the Shu-Osher form, which writes no k-sum) */
 
 /* time integrators (fvhoe/ode.py:245-298) */
 #define FVH_INT_EULER 0
