@@ -142,7 +142,7 @@ struct Smem {
   static constexpr int prim = (DP::A + DP::B) * (int)sizeof(Tc);
   static constexpr int flux = DF::TOTAL * (int)sizeof(Tc);
   static constexpr int detect = (DD::A + DD::B) * (int)sizeof(Tc);
-  static constexpr int fin = (DE::SP + DE::SF + DE::SG) * (int)sizeof(Tc);
+  static constexpr int fin = (DE::SP + DE::SF + DE::SG) * (int)sizeof(Tc) + DE::LIST;
   static constexpr int bytes = f2::Max<f2::Max<prim, flux>::value, f2::Max<detect, fin>::value>::value;
 };
 

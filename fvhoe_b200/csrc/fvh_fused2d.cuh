@@ -1036,6 +1036,10 @@ struct FinalDims {
   static constexpr int SP = PX * PY * 5;
   static constexpr int SF = (TX + 1) * TY * 5;
   static constexpr int SG = TX * (TY + 1) * 5;
+  static constexpr int NXF = (TX + 1) * TY, NYF = TX * (TY + 1);  // faces of the tile
+  // bytes after the three tiles: two counters and the compacted fallback face lists
+  static constexpr int LIST = 16 + 2 * (NXF + NYF);
+  static_assert(NXF < 65536 && NYF < 65536, "face indices are 16-bit");
 };
 
 // RKI < 0: the integrator and stage are read from st at run time.
@@ -1072,10 +1076,16 @@ __device__ __forceinline__ void tile2_final(const double* __restrict__ stage_in,
   // stage input instead of the pointwise tile measured slower: misses touch
   // about one face in seven on KH, too many for scattered loads.
   if (apost && tile_any<TX, TY>(trouble, pred, g, x0, y0)) {
+    // the faces that take the fallback flux, gathered into two lists so that
+    // whole warps solve them: solved in place, a warp holding one such face
+    // among 32 would run the whole MUSCL + Riemann solve for it
+    int* nface = reinterpret_cast<int*>(GY + D::SG);
+    uint16_t* xlist = reinterpret_cast<uint16_t*>(nface + 4);
+    uint16_t* ylist = xlist + D::NXF;
+    if (threadIdx.x == 0) nface[0] = nface[1] = 0;
     pointwise_tile<Tc, TX, TY>(stage_in, g, x0, y0, Pw, ph);
     __syncthreads();
-    // X faces
-    for (int i = threadIdx.x; i < (TX + 1) * TY; i += nt) {
+    for (int i = threadIdx.x; i < D::NXF; i += nt) {
       const int f = i / TY, q = i - f * TY;
       const int x = x0 + f, y = y0 + q;
       if (x > g.nx || y >= g.ny) continue;
@@ -1083,6 +1093,24 @@ __device__ __forceinline__ void tile2_final(const double* __restrict__ stage_in,
       const bool tl = x >= 1 && trouble[ol], trr = x < g.nx && trouble[orr];
       if (!(tl || trr)) continue;
       if (pred && ((x >= 1 && pred[ol]) || (x < g.nx && pred[orr]))) continue;
+      xlist[atomicAdd(&nface[0], 1)] = (uint16_t)i;
+    }
+    for (int i = threadIdx.x; i < D::NYF; i += nt) {
+      const int r = i / (TY + 1), f = i - r * (TY + 1);
+      const int x = x0 + r, y = y0 + f;
+      if (x >= g.nx || y > g.ny) continue;
+      const int ol = x * g.ny + y - 1, orr = x * g.ny + y;
+      const bool tl = y >= 1 && trouble[ol], trr = y < g.ny && trouble[orr];
+      if (!(tl || trr)) continue;
+      if (pred && ((y >= 1 && pred[ol]) || (y < g.ny && pred[orr]))) continue;
+      ylist[atomicAdd(&nface[1], 1)] = (uint16_t)i;
+    }
+    __syncthreads();
+    // X faces
+    const int nx_faces = nface[0], ny_faces = nface[1];
+    for (int k = threadIdx.x; k < nx_faces; k += nt) {
+      const int i = xlist[k];
+      const int f = i / TY, q = i - f * TY;
       Tc flo[5];
       fallback_face_flux<Tc>(Pw + f * D::PY + q + 2, D::PX * D::PY, D::PY, muscl, limiter, ph, g.dx, flo);
 #pragma unroll
@@ -1092,14 +1120,9 @@ __device__ __forceinline__ void tile2_final(const double* __restrict__ stage_in,
       }
     }
     // Y faces
-    for (int i = threadIdx.x; i < TX * (TY + 1); i += nt) {
+    for (int k = threadIdx.x; k < ny_faces; k += nt) {
+      const int i = ylist[k];
       const int r = i / (TY + 1), f = i - r * (TY + 1);
-      const int x = x0 + r, y = y0 + f;
-      if (x >= g.nx || y > g.ny) continue;
-      const int ol = x * g.ny + y - 1, orr = x * g.ny + y;
-      const bool tl = y >= 1 && trouble[ol], trr = y < g.ny && trouble[orr];
-      if (!(tl || trr)) continue;
-      if (pred && ((y >= 1 && pred[ol]) || (y < g.ny && pred[orr]))) continue;
       Tc flo[5];
       fallback_face_flux<Tc>(Pw + (r + 2) * D::PY + f, D::PX * D::PY, 1, muscl, limiter, ph, g.dy, flo);
 #pragma unroll

@@ -700,7 +700,7 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
   // 4. fallback + divergence + Runge-Kutta
   {
     using D = f2::FinalDims<T::EX, T::EY>;
-    const size_t smem = (size_t)(D::SP + D::SF + D::SG) * sizeof(Tc);
+    const size_t smem = (size_t)(D::SP + D::SF + D::SG) * sizeof(Tc) + D::LIST;
     auto kern = f2::final_kernel<Tc, T::EX, T::EY>(c.spec.integrator, c.spec.stage);
     set_smem((const void*)kern, smem);
     const dim3 grid((g.ny + T::EY - 1) / T::EY, (g.nx + T::EX - 1) / T::EX);
