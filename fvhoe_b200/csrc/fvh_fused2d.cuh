@@ -470,6 +470,9 @@ struct FluxDims {
   static constexpr int S1 = Max<AXR * AXS, (TX + 1) * TY>::value * 5 + PAD;
   static constexpr int S2 = Max<AYR * AYS, TX * GYS>::value * 5 + PAD;
   static constexpr int TOTAL = S0 + S1 + S2;  // elements of the compute type
+  // bytes after the three regions that a block with predicted flags needs: two
+  // counters and the lists of the faces that take the fallback flux
+  static constexpr int LIST = 16 + 2 * ((TX + 1) * TY + TX * (TY + 1));
 };
 
 // FW: faces per thread in the Riemann phases (1, 2 or 4): two in FP32, one in
@@ -655,11 +658,19 @@ __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __res
     }
   }
   // predicted cells: their faces take the fallback flux now, blended as the
-  // final pass would (the candidate above keeps the high-order fluxes)
+  // final pass would (the candidate above keeps the high-order fluxes). The
+  // faces are gathered into two lists first so that whole warps solve them
+  // (in place, a warp with one such face would run a full solve for it); the
+  // lists take FluxDims::LIST bytes after the three regions, which a launch
+  // that passes pred allocates.
   if (!pred || !tile_any<TX, TY>(pred, nullptr, g, x0, y0)) return;
   constexpr int PWX = TX + 4, PWY = TY + 4;
   static_assert(PWX * PWY * 5 <= D::S0, "pointwise tile must fit in region 0");
   Tc* Pw = Ws;
+  int* nface = reinterpret_cast<int*>(smem_raw + (size_t)D::TOTAL * sizeof(Tc));
+  uint16_t* xlist = reinterpret_cast<uint16_t*>(nface + 4);
+  uint16_t* ylist = xlist + (TX + 1) * TY;
+  if (threadIdx.x == 0) nface[0] = nface[1] = 0;
   pointwise_tile<Tc, TX, TY>(u, g, x0, y0, Pw, ph);
   __syncthreads();
   for (int i = threadIdx.x; i < (TX + 1) * TY; i += nt) {
@@ -668,11 +679,7 @@ __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __res
     const bool owned = (f < TX || x == g.nx) && x <= g.nx && y < g.ny;
     if (!owned) continue;
     if (!((x >= 1 && pred[(x - 1) * g.ny + y]) || (x < g.nx && pred[x * g.ny + y]))) continue;
-    Tc flo[5];
-    fallback_face_flux<Tc>(Pw + f * PWY + q + 2, PWX * PWY, PWY, muscl, limiter, ph, g.dx, flo);
-    Tc* o = F.p + F.at(x, y);
-#pragma unroll
-    for (int v = 0; v < 5; ++v) o[v * F.vs] = (Tc(1) - Tc(1)) * FX[(v * (TX + 1) + f) * TY + q] + Tc(1) * flo[v];
+    xlist[atomicAdd(&nface[0], 1)] = (uint16_t)i;
   }
   for (int i = threadIdx.x; i < TX * (TY + 1); i += nt) {
     const int r = i / (TY + 1), f = i - r * (TY + 1);
@@ -680,9 +687,25 @@ __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __res
     const bool owned = (f < TY || y == g.ny) && y <= g.ny && x < g.nx;
     if (!owned) continue;
     if (!((y >= 1 && pred[x * g.ny + y - 1]) || (y < g.ny && pred[x * g.ny + y]))) continue;
+    ylist[atomicAdd(&nface[1], 1)] = (uint16_t)i;
+  }
+  __syncthreads();
+  const int nxf = nface[0], nyf = nface[1];
+  for (int k = threadIdx.x; k < nxf; k += nt) {
+    const int i = xlist[k];
+    const int f = i / TY, q = i - f * TY;
+    Tc flo[5];
+    fallback_face_flux<Tc>(Pw + f * PWY + q + 2, PWX * PWY, PWY, muscl, limiter, ph, g.dx, flo);
+    Tc* o = F.p + F.at(x0 + f, y0 + q);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) o[v * F.vs] = (Tc(1) - Tc(1)) * FX[(v * (TX + 1) + f) * TY + q] + Tc(1) * flo[v];
+  }
+  for (int k = threadIdx.x; k < nyf; k += nt) {
+    const int i = ylist[k];
+    const int r = i / (TY + 1), f = i - r * (TY + 1);
     Tc flo[5];
     fallback_face_flux<Tc>(Pw + (r + 2) * PWY + f, PWX * PWY, 1, muscl, limiter, ph, g.dy, flo);
-    Tc* o = G.p + G.at(x, y);
+    Tc* o = G.p + G.at(x0 + r, y0 + f);
 #pragma unroll
     for (int v = 0; v < 5; ++v) o[v * G.vs] = (Tc(1) - Tc(1)) * GY[(v * TX + r) * D::GYS + f] + Tc(1) * flo[v];
   }

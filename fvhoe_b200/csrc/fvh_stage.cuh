@@ -645,7 +645,7 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
   // 2. fluxes (+ candidate)
   {
     using D = f2::FluxDims<P, T::FX, T::FY>;
-    const size_t smem = (size_t)D::TOTAL * sizeof(Tc);
+    const size_t smem = (size_t)D::TOTAL * sizeof(Tc) + (pred ? D::LIST : 0);
     auto kern = f2::k2_fluxes<Tc, P, T::FX, T::FY, KC, KF>;
     set_smem((const void*)kern, smem);
     const dim3 grid((g.ny + T::FY - 1) / T::FY, (g.nx + T::FX - 1) / T::FX);
