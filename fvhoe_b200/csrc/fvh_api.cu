@@ -407,18 +407,34 @@ int read_dt(fvh_handle* h, cudaStream_t s, double* dt_out) {
   return FVH_OK;
 }
 
-// Device copy, copy streams and events of fvh_step_host, made on its first call.
+// Device copy, copy streams and events of fvh_step_host, made on its first
+// call; all or nothing, so a failed set-up is retried by the next call.
 int host_path_init(fvh_handle* h) {
   if (h->host_state) return FVH_OK;
-  const size_t bytes = (size_t)h->nv * h->n[0] * h->n[1] * h->n[2] * sizeof(double);
-  if (int st = alloc(h, (void**)&h->host_state, bytes)) return st;
-  cudaError_t e = cudaStreamCreateWithFlags(&h->copy_in, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->copy_out, cudaStreamNonBlocking);
-  for (int j = 0; j < fvh_handle::kHostChunks && e == cudaSuccess; ++j)
-    e = cudaEventCreateWithFlags(&h->out_done[j], cudaEventDisableTiming);
-  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->in_done, cudaEventDisableTiming);
-  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->step_done, cudaEventDisableTiming);
-  if (e != cudaSuccess) return fail(h, FVH_ERR_CUDA, std::string("host path set-up: ") + cudaGetErrorString(e));
+  cudaStream_t in = nullptr, out = nullptr;
+  cudaEvent_t ev[fvh_handle::kHostChunks + 2] = {};
+  cudaError_t e = cudaStreamCreateWithFlags(&in, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&out, cudaStreamNonBlocking);
+  for (int j = 0; j < fvh_handle::kHostChunks + 2 && e == cudaSuccess; ++j)
+    e = cudaEventCreateWithFlags(&ev[j], cudaEventDisableTiming);
+  double* state = nullptr;
+  int st = FVH_OK;
+  if (e == cudaSuccess)
+    st = alloc(h, (void**)&state, (size_t)h->nv * h->n[0] * h->n[1] * h->n[2] * sizeof(double));
+  if (e != cudaSuccess || st != FVH_OK) {
+    for (cudaEvent_t x : ev)
+      if (x) cudaEventDestroy(x);
+    if (in) cudaStreamDestroy(in);
+    if (out) cudaStreamDestroy(out);
+    if (e != cudaSuccess) return fail(h, FVH_ERR_CUDA, std::string("host path set-up: ") + cudaGetErrorString(e));
+    return st;
+  }
+  h->copy_in = in;
+  h->copy_out = out;
+  for (int j = 0; j < fvh_handle::kHostChunks; ++j) h->out_done[j] = ev[j];
+  h->in_done = ev[fvh_handle::kHostChunks];
+  h->step_done = ev[fvh_handle::kHostChunks + 1];
+  h->host_state = state;
   return FVH_OK;
 }
 

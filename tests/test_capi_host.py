@@ -340,3 +340,10 @@ def test_double_mach_reflection_ic_matches_reference_state(fixture):
                                 tuple(c["h"]), tuple(c["p"]))
     X, Y, Z = fv_uniform_meshgen(tuple(c["n"]), *[tuple(r) for r in c["domain"]])
     assert np.array_equal(u0_fv(X, Y, Z), d["u0"])
+
+
+def test_host_state_entry_points_refuse_null_arguments():
+    from fvhoe_b200 import _capi
+
+    assert _capi.lib.fvh_step_host(None, None, 2, 0.0, 0, 0.0, None, None) == _capi.ERR_ARG
+    assert _capi.lib.fvh_host_sync(None) == _capi.ERR_ARG
