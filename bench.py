@@ -40,8 +40,12 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"],
                     help="the chosen form; fp32 is also compared against the plain fp64 path")
-    ap.add_argument("--accuracy-time", type=float, default=0.01,
-                    help="common time at which the L1 density error against fp64 is taken")
+    ap.add_argument("--accuracy-time", type=float, default=1.0,
+                    help="common time at which the L1 density error against fp64 is taken (the config's t_end)")
+    ap.add_argument("--accuracy-series", default="0.01,0.1,0.5",
+                    help="earlier times at which the L1 density error is also stated (comma-separated)")
+    ap.add_argument("--start-time", type=float, default=0.01,
+                    help="time both forms are advanced to before the timed steps")
     ap.add_argument("--n", type=int, default=2048, help="cells per side")
     ap.add_argument("--p", type=int, default=5)
     ap.add_argument("--e2e-steps", type=int, default=10)
@@ -55,7 +59,7 @@ def parse():
     ap.add_argument("--pred-train-n", type=int, default=1024, help="side of the training runs")
     ap.add_argument("--pred-snapshots", type=int, default=16, help="stages sampled per training run")
     ap.add_argument("--pred-epochs", type=int, default=2)
-    ap.add_argument("--pred-accuracy-time", type=float, default=0.002)
+    ap.add_argument("--pred-accuracy-time", type=float, default=0.02)
     ap.add_argument("--pred-every", type=int, default=3,
                     help="stages between predictions of the second learned form (3: once per SSP-RK3 step)")
     ap.add_argument("--no-sedov", action="store_true", help="skip the 3D Sedov leg")
@@ -210,6 +214,32 @@ def ncu_traffic(kind, n, p, precision):
                 if len(f) == 5 and f[0] == "traffic" and f[1] == key and f[2] == kind:
                     cells = int(f[3].split("=")[1])
                     return int(f[4].split("=")[1]) * (n * n) / cells
+    return None
+
+
+def ncu_stage_traffic(n, p, precision):
+    """DRAM bytes of one whole stage (every launch of the stage) from the line
+    `traffic <precision>_p<p> stage cells=C bytes=B` of the ncu summaries,
+    scaled to n^2 cells."""
+    return ncu_traffic("stage", n, p, precision)
+
+
+# FP64 pipe of a B200: 64 FP64 add / mul / fma per clock per SM, 148 SMs, 1.965 GHz
+FP64_PEAK_OPS = 64 * 148 * 1.965e9
+
+
+def fp64_ops_per_cell(p):
+    """FP64 operations per cell-update of the plain path, counted by ncu from the
+    kernels' executed DADD / DMUL / DFMA instructions (lines
+    `fp64ops fp64_p<p> cells=C ops=O` of the ncu summaries: one stage of C cells)."""
+    import glob
+
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        with open(path) as fh:
+            for line in fh:
+                f = line.split()
+                if len(f) == 4 and f[0] == "fp64ops" and f[1] == f"fp64_p{p}":
+                    return int(f[3].split("=")[1]) / int(f[2].split("=")[1])
     return None
 
 
@@ -580,6 +610,161 @@ def ensemble_leg(args, stream, members=None, label=None):
     }
 
 
+def kernel_profile(lib, _capi, h, step, sp, args, value, precision=None):
+    """Per-kind CUDA-event times of a few steps (each launch bracketed by an event
+    pair) and the roofline of the dominant kind: its algorithmic bytes per
+    launch over its measured duration, against the measured HBM peak; the
+    whole-step fraction of the 120 B per cell-update model; the DRAM traffic per
+    launch and per stage from the committed ncu summaries."""
+    import ctypes
+
+    precision = precision or args.precision
+    _capi.check(lib.fvh_profile_enable(h, 1), h)
+    prof_steps = 3
+    for _ in range(prof_steps):
+        step()
+    K = len(_capi.KERNEL_KINDS)
+    pms = (ctypes.c_double * K)()
+    pbytes = (ctypes.c_double * K)()
+    plaunch = (ctypes.c_uint64 * K)()
+    _capi.check(lib.fvh_profile_read(h, pms, pbytes, plaunch, sp), h)
+    _capi.check(lib.fvh_profile_enable(h, 0), h)
+    total_ms = sum(pms)
+    kinds = {}
+    for i, name in enumerate(_capi.KERNEL_KINDS):
+        if plaunch[i]:
+            kinds[name] = {"ms_per_step": pms[i] / prof_steps, "share": pms[i] / total_ms,
+                           "launches_per_step": plaunch[i] / prof_steps,
+                           "gb_s": pbytes[i] / (pms[i] / 1e3) / 1e9 if pms[i] > 0 else None}
+    dom = max(range(K), key=lambda i: pms[i])
+    dom_name = _capi.KERNEL_KINDS[dom]
+    per_launch_bytes = pbytes[dom] / plaunch[dom]
+    per_launch_s = pms[dom] / plaunch[dom] / 1e3
+    achieved = per_launch_bytes / per_launch_s / 1e9
+    peak, peak_src = hbm_peak()
+    traffic = ncu_traffic(dom_name, args.n, args.p, precision)
+    step_gbs = 120 * value * 1e6 / 1e9
+    stage = ncu_stage_traffic(args.n, args.p, precision)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": dom_name, "peak_source": f"{peak_src} HBM copy bandwidth",
+                "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_s * 1e3,
+                "step_frac": step_gbs / peak,
+                "stage_model": {"bytes_per_cell_update": 120, "achieved_gb_s": step_gbs},
+                "dram_bytes_per_stage": stage,
+                "dram_over_algorithmic": stage / (120.0 * args.n * args.n) if stage else None}
+    fp64 = fp64_ops_per_cell(args.p) if precision == "fp64" else None
+    if fp64:
+        rate = fp64 * value * 1e6  # FP64 operations per second at this throughput
+        roofline["fp64"] = {"ops_per_cell_update": fp64, "achieved_tops": rate / 1e12,
+                            "peak_tops": FP64_PEAK_OPS / 1e12, "frac": rate / FP64_PEAK_OPS,
+                            "peak_model": "64 FP64 add/mul/fma per clock per SM x 148 SMs x 1.965 GHz "
+                                          "(the FP64 pipe; no FMA contraction in the plain path)"}
+    return kinds, roofline
+
+
+def e2e_leg(lib, _capi, h, u, sp, stream, args, cells, world, dist):
+    """End to end through the C ABI with the state in pinned host memory: every
+    step copies the whole state in, steps it (dt read back) and copies it out.
+    fvh_step_host pipelines the copies in chunks (a step's copy-out overlaps the
+    next step's copy-in); the serial form (copy in, step, copy out, wait) is
+    timed too for comparison."""
+    import ctypes
+
+    import torch
+
+    host = torch.empty(u.shape, dtype=torch.float64, pin_memory=True)
+    host.copy_(u)
+    torch.cuda.synchronize()
+    nbytes = u.numel() * 8
+    dt = ctypes.c_double()
+    ssprk3 = _capi.INTEGRATOR["ssprk3"]
+    hptr = ctypes.c_void_p(host.data_ptr())
+    uptr = ctypes.c_void_p(u.data_ptr())
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        _capi.check(lib.fvh_set_log_mode(h, 1), h)
+        _capi.check(lib.fvh_set_log_divisor(h, 3.0), h)
+        _capi.check(lib.fvh_step_host(h, hptr, ssprk3, 0.0, 0, 0.0, ctypes.byref(dt), sp), h)
+    _capi.check(lib.fvh_host_sync(h), h)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        u.copy_(host, non_blocking=True)
+        _capi.check(lib.fvh_set_log_mode(h, 1), h)
+        _capi.check(lib.fvh_set_log_divisor(h, 3.0), h)
+        _capi.check(lib.fvh_step(h, uptr, ssprk3, 0.0, 0, 0.0, ctypes.byref(dt), sp), h)
+        host.copy_(u, non_blocking=True)
+        stream.synchronize()
+    serial_s = max_over_ranks(time.perf_counter() - t0, dist)
+    return {"value": world * 3 * cells * args.e2e_steps / e2e_s / 1e6, "unit": UNIT,
+            "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": args.e2e_steps,
+            "path": "fvh_step_host through the C ABI: state in pinned host memory, copied in and out every "
+                    "step in 16 chunks on two copy streams",
+            "serial_value": world * 3 * cells * args.e2e_steps / serial_s / 1e6}
+
+
+def accuracy_run(args, series, seed, stream):
+    """The chosen form and plain FP64 from the same initial state to each time of
+    `series` in turn (EulerSolver.ssprk3 with exact target hits, as the
+    reference's integrate does): the L1 density error at every time, and each
+    form's whole-run throughput (CUDA events around each segment, host loop
+    and dt read-backs included)."""
+    import torch
+
+    from fvhoe_b200 import EulerSolver
+
+    cells = args.n * args.n
+    out = {"t": series[-1], "definition": "mean |rho_chosen - rho_fp64| over the grid at time t, same initial "
+                                          "state, each form with its own CFL steps and exact target hits",
+           "series": []}
+    solvers = {"chosen": EulerSolver(precision=args.precision, **solver_kwargs(args.n, args.p, seed=seed)),
+               "fp64": EulerSolver(precision="fp64", **solver_kwargs(args.n, args.p, seed=seed))}
+    run_ms = {k: 0.0 for k in solvers}
+    for t in series:
+        for name, sv in solvers.items():
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            sv.ssprk3(t)
+            b.record(stream)
+            torch.cuda.synchronize()
+            run_ms[name] += a.elapsed_time(b)
+        rho_c = solvers["chosen"].am("u")[0]
+        rho_p = solvers["fp64"].am("u")[0]
+        out["series"].append({"t": t, "l1": float(torch.mean(torch.abs(rho_c - rho_p)).item()),
+                              "steps_chosen": solvers["chosen"].step_count,
+                              "steps_fp64": solvers["fp64"].step_count})
+    out["value"] = out["series"][-1]["l1"]
+    out["whole_run"] = {name: {"mcell_updates_per_s": 3 * cells * sv.step_count / (run_ms[name] / 1e3) / 1e6,
+                               "steps": sv.step_count, "seconds": run_ms[name] / 1e3}
+                        for name, sv in solvers.items()}
+    out["whole_run"]["speedup_of_chosen"] = (out["whole_run"]["chosen"]["mcell_updates_per_s"] /
+                                             out["whole_run"]["fp64"]["mcell_updates_per_s"])
+    del solvers
+    torch.cuda.empty_cache()
+    return out
+
+
+def leg_summary(legs):
+    """The few figures of each leg that the headline line repeats."""
+    out = {}
+    lp = legs.get("learned_predictor")
+    if lp:
+        out["learned_predictor"] = ({k: lp[k] for k in ("config", "mcell_updates_per_s", "speedup_vs_plain_fp64")}
+                                    if "error" not in lp else lp)
+        if "l1_density_error_vs_fp64" in lp:
+            out["learned_predictor"]["l1"] = lp["l1_density_error_vs_fp64"]
+    sd = legs.get("sedov_3d")
+    if sd:
+        out["sedov_3d"] = ({k: sd[k]["mcell_updates_per_s"] for k in ("fp64", "fp32")} if "error" not in sd else sd)
+    be = legs.get("batched_ensemble")
+    if be:
+        out["batched_ensemble"] = ({"value": be["value"], "batching_gain": be["batching_gain"],
+                                    "small_members_gain": be.get("small_members", {}).get("batching_gain")}
+                                   if "error" not in be else be)
+    return out
+
+
 def run_ours(args):
     import ctypes
 
@@ -595,22 +780,15 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
     sp = ctypes.c_void_p(stream.cuda_stream)
 
-    # the chosen form and the plain FP64 path on the same initial state; both are first
-    # advanced to a common time with the reference's stepper (exact target hit) to state
-    # the L1 density error of the chosen form against FP64
+    # the chosen form and the plain FP64 path on the same initial state, both first
+    # advanced to t = 0.01 with the reference's stepper (the state the timed steps start from)
+    t_start = args.start_time
     chosen = EulerSolver(precision=args.precision, **solver_kwargs(args.n, args.p, seed=rank))
-    plain = EulerSolver(precision="fp64", **solver_kwargs(args.n, args.p, seed=rank)) \
-        if args.precision != "fp64" and not args.no_plain else None
-    t_acc = args.accuracy_time
-    chosen.ssprk3(t_acc)
-    l1 = {"value": 0.0, "t": t_acc, "steps_chosen": chosen.step_count}
-    if plain is not None:
-        plain.ssprk3(t_acc)
-        rho_c = chosen.am("u")[0]
-        rho_p = plain.am("u")[0]
-        l1 = {"value": float(torch.mean(torch.abs(rho_c - rho_p)).item()), "t": t_acc,
-              "steps_chosen": chosen.step_count, "steps_fp64": plain.step_count,
-              "definition": "mean |rho_chosen - rho_fp64| over the grid at time t, same initial state"}
+    chosen.ssprk3(t_start)
+    plain = None
+    if args.precision != "fp64" and not args.no_plain:
+        plain = EulerSolver(precision="fp64", **solver_kwargs(args.n, args.p, seed=rank))
+        plain.ssprk3(t_start)
 
     h = chosen._handle
     u = chosen.am("u")
@@ -642,110 +820,77 @@ def run_ours(args):
         msp, _ = _time_steps(lib, _capi, hp, up, sp, stream, args.steps)
         pv, msp = replica_throughput(3 * cells * args.steps, msp, dist, world)
         plain_line = {"value": pv, "ms_per_step": msp / args.steps, "speedup_of_chosen": value / pv}
-        del plain
 
     # per-kernel timing of a few steps for the roofline of the dominant kernel
-    _capi.check(lib.fvh_profile_enable(h, 1), h)
-    prof_steps = 3
-    for _ in range(prof_steps):
-        step()
-    K = len(_capi.KERNEL_KINDS)
-    pms = (ctypes.c_double * K)()
-    pbytes = (ctypes.c_double * K)()
-    plaunch = (ctypes.c_uint64 * K)()
-    _capi.check(lib.fvh_profile_read(h, pms, pbytes, plaunch, sp), h)
-    _capi.check(lib.fvh_profile_enable(h, 0), h)
-    total_ms = sum(pms)
-    kinds = {}
-    for i, name in enumerate(_capi.KERNEL_KINDS):
-        if plaunch[i]:
-            kinds[name] = {"ms_per_step": pms[i] / prof_steps, "share": pms[i] / total_ms,
-                           "launches_per_step": plaunch[i] / prof_steps,
-                           "gb_s": pbytes[i] / (pms[i] / 1e3) / 1e9 if pms[i] > 0 else None}
-    dom = max(range(K), key=lambda i: pms[i])
-    dom_name = _capi.KERNEL_KINDS[dom]
-    per_launch_bytes = pbytes[dom] / plaunch[dom]
-    per_launch_s = pms[dom] / plaunch[dom] / 1e3
-    achieved = per_launch_bytes / per_launch_s / 1e9
-    peak, peak_src = hbm_peak()
-    traffic = ncu_traffic(dom_name, args.n, args.p, args.precision)
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": dom_name, "peak_source": f"{peak_src} HBM copy bandwidth",
-                "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_s * 1e3,
-                "stage_model": {"bytes_per_cell_update": 120,
-                                "achieved_gb_s": 120 * value / world * 1e6 / 1e9}}
+    kinds, roofline = kernel_profile(lib, _capi, h, step, sp, args, value / world)
+    if plain is not None:
+        _, pstep = _time_steps(lib, _capi, hp, up, sp, stream, 0)
+        pkinds, proof = kernel_profile(lib, _capi, hp, pstep, sp, args, plain_line["value"] / world, precision="fp64")
+        plain_line["roofline"] = {k: proof[k] for k in ("kernel", "frac", "step_frac", "dram_over_algorithmic")}
+        if "fp64" in proof:
+            plain_line["roofline"]["fp64"] = {k: proof["fp64"][k] for k in ("ops_per_cell_update", "achieved_tops",
+                                                                              "frac")}
 
-    # end to end through the C ABI with the state in pinned host memory: every step
-    # copies the whole state in, steps it (dt read back) and copies it out.
-    # fvh_step_host pipelines the copies in chunks (a step's copy-out overlaps the
-    # next step's copy-in); the serial form (copy in, step, copy out, wait) is
-    # timed too for comparison.
-    host = torch.empty(u.shape, dtype=torch.float64, pin_memory=True)
-    host.copy_(u)
-    torch.cuda.synchronize()
-    nbytes = u.numel() * 8
-    dt = ctypes.c_double()
-    ssprk3 = _capi.INTEGRATOR["ssprk3"]
-    hptr = ctypes.c_void_p(host.data_ptr())
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
-        _capi.check(lib.fvh_set_log_mode(h, 1), h)
-        _capi.check(lib.fvh_set_log_divisor(h, 3.0), h)
-        _capi.check(lib.fvh_step_host(h, hptr, ssprk3, 0.0, 0, 0.0, ctypes.byref(dt), sp), h)
-    _capi.check(lib.fvh_host_sync(h), h)
-    e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
-        u.copy_(host, non_blocking=True)
-        _capi.check(lib.fvh_set_log_mode(h, 1), h)
-        _capi.check(lib.fvh_set_log_divisor(h, 3.0), h)
-        _capi.check(lib.fvh_step(h, uptr, ssprk3, 0.0, 0, 0.0, ctypes.byref(dt), sp), h)
-        host.copy_(u, non_blocking=True)
-        stream.synchronize()
-    serial_s = max_over_ranks(time.perf_counter() - t0, dist)
-    e2e = {"value": world * 3 * cells * args.e2e_steps / e2e_s / 1e6, "unit": UNIT,
-           "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": args.e2e_steps,
-           "path": "fvh_step_host through the C ABI: state in pinned host memory, copied in and out every "
-                   "step in 16 chunks on two copy streams",
-           "serial_value": world * 3 * cells * args.e2e_steps / serial_s / 1e6}
-
+    # end to end through the C ABI with the state in pinned host memory
+    e2e = e2e_leg(lib, _capi, h, u, sp, stream, args, cells, world, dist)
+    if plain is not None:
+        pe = e2e_leg(lib, _capi, hp, plain.am("u"), sp, stream, args, cells, world, dist)
+        plain_line["e2e"] = {k: pe[k] for k in ("value", "unit", "serial_value")}
+        del plain
     stats = chosen.stats()
+    del chosen
+    torch.cuda.empty_cache()
+
+    # L1 density error of the chosen form against plain FP64 at the config's t_end
+    # (fresh solvers, the same stepper and targets), with the whole-run throughput
+    l1 = None
+    if args.precision != "fp64" and not args.no_plain and world == 1:
+        series = [float(x) for x in args.accuracy_series.split(",") if x] + [args.accuracy_time]
+        l1 = accuracy_run(args, series, seed=rank, stream=stream)
+
     if rank == 0:
         form = {"fp32": "FP32 reconstruction, Riemann fluxes and detection; FP64 stage accumulation",
                 "fp64": "plain FP64, bit-exact with the reference"}[args.precision]
+        legs = {}
+        if world == 1 and not args.no_predictor:
+            torch.cuda.empty_cache()
+            try:
+                legs["learned_predictor"] = predictor_leg(args, stream, sp)
+            except Exception as exc:  # the headline line is printed whatever this leg does
+                legs["learned_predictor"] = {"error": f"{type(exc).__name__}: {exc}"}
+        if world == 1 and not args.no_sedov:
+            torch.cuda.empty_cache()
+            try:
+                legs["sedov_3d"] = sedov_leg(args, stream, sp)
+            except Exception as exc:
+                legs["sedov_3d"] = {"error": f"{type(exc).__name__}: {exc}"}
+        if world == 1 and not args.no_ensemble:
+            torch.cuda.empty_cache()
+            try:
+                legs["batched_ensemble"] = ensemble_leg(args, stream)
+                # where batching pays: many small members, launch- and host-bound one at a time
+                legs["batched_ensemble"]["small_members"] = ensemble_leg(
+                    args, stream, ensemble_members(args.ens_members, side=128), "all of side 128")
+            except Exception as exc:
+                legs["batched_ensemble"] = {"error": f"{type(exc).__name__}: {exc}"}
+        # every leg in full on its own line, then the headline line last (compact)
+        for name, leg in legs.items():
+            print(f"leg {name} " + json.dumps(leg), flush=True)
+        if kinds:
+            print("leg kernels " + json.dumps(kinds), flush=True)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32", "data": "synthetic",
-            "config": dict(workload_config(args), parallelism=f"replicas x{world}" if world > 1 else "single"),
-            "chosen_form": form, "plain_fp64": plain_line, "l1_density_error_vs_fp64": l1,
-            "roofline": roofline, "kernels": kinds, "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
+            "plain_fp64": plain_line, "l1_density_error_vs_fp64": l1,
+            "config": dict(workload_config(args), parallelism=f"replicas x{world}" if world > 1 else "single",
+                           timed_from=f"t = {t_start} (both forms advanced there first)"),
+            "chosen_form": form, "roofline": roofline, "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
             "troubled_cells_last_stage": stats["troubled"], "nonfinite": stats["nonfinite"],
+            "legs": leg_summary(legs),
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_port(args)
-        if world == 1 and not args.no_predictor:
-            del chosen
-            torch.cuda.empty_cache()
-            try:
-                line["learned_predictor"] = predictor_leg(args, stream, sp)
-            except Exception as exc:  # the headline line is printed whatever this leg does
-                line["learned_predictor"] = {"error": f"{type(exc).__name__}: {exc}"}
-        if world == 1 and not args.no_sedov:
-            torch.cuda.empty_cache()
-            try:
-                line["sedov_3d"] = sedov_leg(args, stream, sp)
-            except Exception as exc:
-                line["sedov_3d"] = {"error": f"{type(exc).__name__}: {exc}"}
-        if world == 1 and not args.no_ensemble:
-            torch.cuda.empty_cache()
-            try:
-                line["batched_ensemble"] = ensemble_leg(args, stream)
-                # where batching pays: many small members, launch- and host-bound one at a time
-                line["batched_ensemble"]["small_members"] = ensemble_leg(
-                    args, stream, ensemble_members(args.ens_members, side=128), "all of side 128")
-            except Exception as exc:
-                line["batched_ensemble"] = {"error": f"{type(exc).__name__}: {exc}"}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -36,6 +36,7 @@ EXPORTS = (
     "fvh_scratch_bytes",
     "fvh_rhs",
     "fvh_step",
+    "fvh_stage",
     "fvh_step_host",
     "fvh_host_sync",
     "fvh_primitives",
@@ -81,6 +82,7 @@ EXPORTS = (
     "fvh_ensemble_variant_info",
     "fvh_ensemble_autotune",
     "fvh_ensemble_graph_info",
+    "fvh_ensemble_set_wait_limit",
 )
 
 KERNEL_KINDS = ("centre", "transverse", "face", "candidate", "detect", "fallback", "final", "small", "predict")
@@ -170,6 +172,8 @@ def _load():
     lib.fvh_scratch_bytes.restype = ctypes.c_size_t
     lib.fvh_rhs.argtypes = [vp, vp, vp, dp, vp]
     lib.fvh_step.argtypes = [vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, dp, vp]
+    lib.fvh_stage.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                              dp, vp]
     lib.fvh_step_host.argtypes = [vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, dp, vp]
     lib.fvh_host_sync.argtypes = [vp]
     lib.fvh_primitives.argtypes = [vp, vp, vp, ctypes.c_int, vp]
@@ -231,12 +235,13 @@ def _load():
     lib.fvh_ensemble_variant_info.argtypes = [vp, ctypes.c_int, ip, ip, ip, ctypes.POINTER(ctypes.c_size_t)]
     lib.fvh_ensemble_autotune.argtypes = [vp, ctypes.c_int, ip, ip, dp, vp]
     lib.fvh_ensemble_graph_info.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_char_p)]
+    lib.fvh_ensemble_set_wait_limit.argtypes = [vp, ctypes.c_uint]
     for name in ("fvh_ensemble_create", "fvh_ensemble_destroy", "fvh_ensemble_load", "fvh_ensemble_store",
                  "fvh_ensemble_reset", "fvh_ensemble_step",
                  "fvh_ensemble_status", "fvh_ensemble_configure", "fvh_ensemble_variant_info",
-                 "fvh_ensemble_autotune", "fvh_ensemble_graph_info"):
+                 "fvh_ensemble_autotune", "fvh_ensemble_graph_info", "fvh_ensemble_set_wait_limit"):
         getattr(lib, name).restype = ctypes.c_int
-    for name in ("fvh_create", "fvh_destroy", "fvh_rhs", "fvh_step", "fvh_step_host", "fvh_host_sync",
+    for name in ("fvh_create", "fvh_destroy", "fvh_rhs", "fvh_step", "fvh_stage", "fvh_step_host", "fvh_host_sync",
                  "fvh_primitives", "fvh_trouble_flags",
                  "fvh_trouble_log", "fvh_set_log_mode", "fvh_get_stats", "fvh_profile_enable", "fvh_profile_read",
                  "fvh_mlp_create", "fvh_mlp_destroy", "fvh_mlp_get_params", "fvh_mlp_set_params", "fvh_mlp_features",
@@ -257,10 +262,16 @@ class FvhError(RuntimeError):
         self.status = status
 
 
+class FvhNonFiniteError(FvhError, FloatingPointError):
+    """FVH_ERR_NONFINITE: the update wrote NaN/Inf values, or its time step is
+    not finite or not positive."""
+
+
 def check(status: int, handle=None) -> None:
     if status != OK:
         msg = lib.fvh_last_error(handle)
-        raise FvhError(status, msg.decode() if msg else "")
+        cls = FvhNonFiniteError if status == ERR_NONFINITE else FvhError
+        raise cls(status, msg.decode() if msg else "")
 
 
 def default_config() -> FvhConfig:

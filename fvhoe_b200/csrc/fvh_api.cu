@@ -230,6 +230,11 @@ int configure(fvh_handle* h, const fvh_config* cfg, std::string& msg) {
     msg = "grid too large: a sweep buffer would exceed 2^31 elements";
     return FVH_ERR_CONFIG;
   }
+  return FVH_OK;
+}
+
+// cfg->device must name a visible CUDA device.
+int check_device(const fvh_config* cfg, std::string& msg) {
   int count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess) {
     cudaGetLastError();
@@ -377,8 +382,10 @@ int allocate(fvh_handle* h) {
 }  // namespace
 
 namespace fvh {
-// Configuration checks shared with the handle-free entry point (fvh_noalloc.cu).
+// Configuration checks shared with the handle-free entry point (fvh_noalloc.cu):
+// the geometry and kinds of cfg (no CUDA call), and the device ordinal.
 int configure_handle(fvh_handle* h, const fvh_config* cfg, std::string& msg) { return configure(h, cfg, msg); }
+int check_device_visible(const fvh_config* cfg, std::string& msg) { return check_device(cfg, msg); }
 }  // namespace fvh
 
 namespace {
@@ -394,6 +401,11 @@ int next_log_mode(fvh_handle* h) {
   return m;
 }
 
+// The dt read-back of fvh_step / fvh_rhs / fvh_step_host. The same copy brings
+// the step's non-finite count, so a call that reads dt also reports a failed
+// update: FVH_ERR_NONFINITE when the update wrote NaN/Inf values, when dt is
+// not finite, or when a CFL dt is not positive (an infinite signal speed);
+// *dt_out is written in every case.
 int read_dt(fvh_handle* h, cudaStream_t s, double* dt_out) {
   if (!dt_out) return FVH_OK;
   fvh::Scalars host{};
@@ -404,6 +416,13 @@ int read_dt(fvh_handle* h, cudaStream_t s, double* dt_out) {
     return FVH_ERR_CUDA;
   }
   *dt_out = host.dt_step;
+  if (host.nonfinite)
+    return fail(h, FVH_ERR_NONFINITE,
+                "the update wrote " + std::to_string(host.nonfinite) + " non-finite values");
+  if (!std::isfinite(host.dt_step) || !std::isfinite(host.dt_stage))
+    return fail(h, FVH_ERR_NONFINITE, "the time step is not finite");
+  if (!h->cfg.use_fixed_dt && !(host.dt_stage > 0.0))
+    return fail(h, FVH_ERR_NONFINITE, "the CFL time step is not positive (infinite signal speed)");
   return FVH_OK;
 }
 
@@ -490,6 +509,7 @@ int fvh_create(const fvh_config* cfg, fvh_handle** out) {
   }
   std::string msg;
   int st = configure(h, cfg, msg);
+  if (!st) st = check_device(cfg, msg);
   if (st) {
     g_create_error = msg;
     delete h;
@@ -540,45 +560,76 @@ int fvh_rhs(fvh_handle* h, const double* u, double* dudt, double* dt_out, void* 
   return read_dt(h, s, dt_out);
 }
 
+namespace {
+
+int stage_count(int integrator) {
+  switch (integrator) {
+    case FVH_INT_EULER: return 1;
+    case FVH_INT_SSPRK2: return 2;
+    case FVH_INT_SSPRK3: return 3;
+    case FVH_INT_RK4: return 4;
+    default: return 0;
+  }
+}
+
+// Stage k of a step of u. Stage inputs: u, then alternating S[0], S[1]; the
+// last stage writes u.
+int step_stage(fvh_handle* h, double* u, int integrator, int k, int stages, double t, int has_target,
+               double target, cudaStream_t s) {
+  fvh::StageCall c{};
+  const double* in = k == 0 ? u : h->S[(k - 1) & 1];
+  c.stage_in = in;
+  c.spec.integrator = integrator;  // FVH_INT_* and fvh::Integrator share values
+  c.spec.stage = k;
+  c.spec.stage_in = in;
+  c.spec.u = u;
+  c.spec.acc = h->acc;
+  c.spec.next = h->S[k & 1];
+  c.first_stage = k == 0;
+  c.has_target = has_target;
+  c.t = t;
+  c.target = target;
+  c.log_mode = next_log_mode(h);
+  c.log_div = k == stages - 1 ? h->log_divisor : 0.0;
+  const int st = run_stage(h, c, s);
+  if (st || k == stages - 1) h->log_divisor = 0.0;
+  return st;
+}
+
+}  // namespace
+
 int fvh_step(fvh_handle* h, double* u, int integrator, double t, int has_target, double target, double* dt_out,
              void* stream) {
   if (!h) return FVH_ERR_ARG;
   if (!u) return fail(h, FVH_ERR_ARG, "null array");
-  int stages;
-  switch (integrator) {
-    case FVH_INT_EULER: stages = 1; break;
-    case FVH_INT_SSPRK2: stages = 2; break;
-    case FVH_INT_SSPRK3: stages = 3; break;
-    case FVH_INT_RK4: stages = 4; break;
-    default: return fail(h, FVH_ERR_ARG, "unknown integrator");
-  }
+  const int stages = stage_count(integrator);
+  if (!stages) return fail(h, FVH_ERR_ARG, "unknown integrator");
   if (int st0 = use_device(h)) return st0;
   cudaStream_t s = (cudaStream_t)stream;
-  // stage inputs: u, then alternating S[0], S[1]
-  const double* in = u;
-  for (int k = 0; k < stages; ++k) {
-    fvh::StageCall c{};
-    c.stage_in = in;
-    c.spec.integrator = integrator;  // FVH_INT_* and fvh::Integrator share values
-    c.spec.stage = k;
-    c.spec.stage_in = in;
-    c.spec.u = u;
-    c.spec.acc = h->acc;
-    c.spec.next = h->S[k & 1];
-    c.first_stage = k == 0;
-    c.has_target = has_target;
-    c.t = t;
-    c.target = target;
-    c.log_mode = next_log_mode(h);
-    c.log_div = k == stages - 1 ? h->log_divisor : 0.0;
-    const int st = run_stage(h, c, s);
-    if (st) {
-      h->log_divisor = 0.0;
-      return st;
-    }
-    in = h->S[k & 1];
-  }
-  h->log_divisor = 0.0;
+  h->next_stage = 0;
+  for (int k = 0; k < stages; ++k)
+    if (int st = step_stage(h, u, integrator, k, stages, t, has_target, target, s)) return st;
+  return read_dt(h, s, dt_out);
+}
+
+int fvh_stage(fvh_handle* h, double* u, int integrator, int k, double t, int has_target, double target,
+              double* dt_out, void* stream) {
+  if (!h) return FVH_ERR_ARG;
+  if (!u) return fail(h, FVH_ERR_ARG, "null array");
+  const int stages = stage_count(integrator);
+  if (!stages) return fail(h, FVH_ERR_ARG, "unknown integrator");
+  if (k < 0 || k >= stages) return fail(h, FVH_ERR_ARG, "stage index out of range for this integrator");
+  if (k != 0 && (k != h->next_stage || integrator != h->stage_integrator || u != h->stage_state))
+    return fail(h, FVH_ERR_ARG,
+                "stage " + std::to_string(k) + " must follow stage " + std::to_string(k - 1) +
+                    " of the same integrator and state");
+  if (int st0 = use_device(h)) return st0;
+  cudaStream_t s = (cudaStream_t)stream;
+  h->next_stage = 0;
+  if (int st = step_stage(h, u, integrator, k, stages, t, has_target, target, s)) return st;
+  h->next_stage = k + 1 < stages ? k + 1 : 0;
+  h->stage_integrator = integrator;
+  h->stage_state = u;
   return read_dt(h, s, dt_out);
 }
 

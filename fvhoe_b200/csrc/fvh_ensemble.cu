@@ -15,6 +15,7 @@
 
 namespace fvh {
 int configure_handle(fvh_handle* h, const fvh_config* cfg, std::string& msg);
+int check_device_visible(const fvh_config* cfg, std::string& msg);
 }
 
 using namespace fvh;
@@ -175,6 +176,13 @@ int fvh_ensemble_create(const fvh_config* cfg, int nprob, const int* nx, const i
     e->ny.push_back(ny[q]);
     e->hx.push_back(hx[q]);
     e->hy.push_back(hy[q]);
+  }
+  {
+    std::string msg;
+    if (int st = fvh::check_device_visible(&e->cfg, msg)) {
+      delete e;
+      return fail(nullptr, st, msg);
+    }
   }
   if (cudaSetDevice(e->cfg.device) != cudaSuccess) {
     delete e;
@@ -392,6 +400,14 @@ int fvh_ensemble_configure(fvh_ensemble* e, int variant, int blocks_per_sm, int 
   e->use_graph = use_graph != 0;
   drop_graph(e);
   return upload(e, nullptr);
+}
+
+int fvh_ensemble_set_wait_limit(fvh_ensemble* e, unsigned int polls) {
+  if (!e) return FVH_ERR_ARG;
+  if (polls == e->wait_limit) return FVH_OK;
+  e->wait_limit = polls;
+  drop_graph(e);  // a captured step holds the old bound in its kernel arguments
+  return FVH_OK;
 }
 
 int fvh_ensemble_variant_info(fvh_ensemble* e, int variant, int* tx, int* ty, int* max_blocks_per_sm,

@@ -73,12 +73,16 @@ struct Args {
   Phys<Tc> ph;
   DetectSpec ds;
   Barrier* bar;
+  unsigned int wait_limit;  // polls a barrier wait makes before it gives up
   unsigned int* active_count;
 };
 
+// Default barrier wait bound: 2^24 polls (seconds with the back-off below).
+constexpr unsigned int kDefaultWaitLimit = 1u << 24;
+
 // Bounded grid barrier (all blocks resident: cooperative launch). Returns
 // false when the wait gave up or another block aborted.
-__device__ __forceinline__ bool grid_barrier(Barrier* b) {
+__device__ __forceinline__ bool grid_barrier(Barrier* b, unsigned int limit) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -94,7 +98,6 @@ __device__ __forceinline__ bool grid_barrier(Barrier* b) {
       atomicAdd(&b->gen, 1u);
     } else {
       unsigned int i = 0;
-      const unsigned int limit = 1u << 24;  // ~ seconds with the back-off below
       while (*vgen == g && *vabort == 0u && i < limit) {
         __nanosleep(64);
         ++i;
@@ -170,7 +173,7 @@ __global__ void __launch_bounds__(256)
         stage_input(p, stage), g, f2::make_v2((Tc*)p->W, g.nx, g.ny, a.gW), a.gW, a.crule, a.trule, a.ph, rs, p->sc,
         li % p->tiles_y[0], li / p->tiles_y[0], smem_raw);
   }
-  if (!grid_barrier(a.bar)) return;
+  if (!grid_barrier(a.bar, a.wait_limit)) return;
   // dt of the step (stage 1): the CFL dt clamped to the target
   if (stage == 0 && blockIdx.x == 0) {
     for (int q = threadIdx.x; q < a.nprob; q += blockDim.x) {
@@ -195,7 +198,7 @@ __global__ void __launch_bounds__(256)
                                             a.crule, a.trule, a.lrule, a.rrule, a.ph, p->cx, p->cy, dt, nullptr, 1,
                                             a.limiter, li % p->tiles_y[1], li / p->tiles_y[1], smem_raw);
   }
-  if (!grid_barrier(a.bar)) return;
+  if (!grid_barrier(a.bar, a.wait_limit)) return;
   // ---- phase 3: a-posteriori detection
   if (a.apost) {
     for (int i = blockIdx.x; i < a.ntiles[2]; i += gridDim.x) {
@@ -209,7 +212,7 @@ __global__ void __launch_bounds__(256)
       f2::tile2_detect<Tc, P, TX, TY, KC>((const Tc*)p->us, g, Wc, a.crule, a.trule, a.ph, a.ds, p->sc, p->trouble, nullptr,
                                           nullptr, nullptr, li % p->tiles_y[2], li / p->tiles_y[2], smem_raw);
     }
-    if (!grid_barrier(a.bar)) return;
+    if (!grid_barrier(a.bar, a.wait_limit)) return;
   }
   // ---- phase 4: fallback, divergence, Runge-Kutta combination
   for (int i = blockIdx.x; i < a.ntiles[3]; i += gridDim.x) {
@@ -231,7 +234,7 @@ __global__ void __launch_bounds__(256)
     f2::tile2_final<Tc, TX, TY>(st.stage_in, g, Fc, Gc, p->trouble, nullptr, a.apost, 1, a.limiter, a.ph, p->cx, p->cy,
                                 st, p->dt_step, p->sc, li % p->tiles_y[3], li / p->tiles_y[3], smem_raw);
   }
-  if (!grid_barrier(a.bar)) return;
+  if (!grid_barrier(a.bar, a.wait_limit)) return;
   // ---- end of stage: fresh reductions for the next stage; the last stage advances time
   if (blockIdx.x == 0) {
     unsigned int active = 0;

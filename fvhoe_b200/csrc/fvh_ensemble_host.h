@@ -41,6 +41,7 @@ struct fvh_ensemble {
   size_t arena_bytes = 0;
   fvh::ens::Barrier* bar = nullptr;
   unsigned int* active_count = nullptr;
+  unsigned int wait_limit = 0;         // barrier polls before a wait gives up (0 = the default)
   int variant = 0;
   int blocks_per_sm = 0;               // 0 = as many as fit
   bool use_graph = true;

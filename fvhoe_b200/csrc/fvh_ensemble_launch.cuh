@@ -93,6 +93,7 @@ int launch_t(fvh_ensemble* e, int stage, int last, cudaStream_t s) {
   ds.log_mode = 0;
   a.ds = ds;
   a.bar = e->bar;
+  a.wait_limit = e->wait_limit ? e->wait_limit : kDefaultWaitLimit;
   a.active_count = e->active_count;
   void* params[] = {&a};
   LaunchScope scope(KK_FINAL, 0.0, s);

@@ -64,6 +64,9 @@ struct fvh_handle {
   cudaEvent_t in_done = nullptr, step_done = nullptr;
   bool out_pending = false;       // out_done events recorded by an earlier call
   int log_mode_next = 1;          // log mode of the next stage
+  int next_stage = 0;             // fvh_stage: the stage the next call must run (0 = a new step)
+  int stage_integrator = -1;      // fvh_stage: integrator and state of the step in progress
+  const double* stage_state = nullptr;
   double log_divisor = 0.0;       // divisor applied by the next step's last stage (one-shot)
   fvh::Profiler* prof = nullptr;  // per-launch timing, when enabled
   fvh::KernelTotals prof_totals{};

@@ -87,13 +87,31 @@ __device__ __forceinline__ bool publish_operands() {
 
 // All threads: wait (bounded) for the GEMMs committed to bar. Returns false in
 // every thread of the block when any thread gave up; the caller then stops
-// issuing (the error counter tells the host).
+// issuing and releases TMEM (the error counter tells the host).
+//
+// Give-up path: a commit whose wait ran out may still be executing, and its
+// MMAs write TMEM and its completion arrives on `bar` in this CTA's shared
+// memory. Releasing TMEM (or ending the CTA, which hands its shared memory to
+// the next CTA) before they land would let them write memory that is no
+// longer this CTA's. So on a give-up every thread first drains: it waits
+// again, with a 16x longer bound, for the same phase. Once that phase has
+// completed no MMA of this CTA is in flight (each commit tracks all MMAs the
+// thread issued before it, and nothing is issued after a give-up), and the
+// release is safe. If the drain runs out too, the block still releases and
+// returns, so the kernel ends instead of hanging, and the second count tells
+// the host that the last commit never completed.
 __device__ __forceinline__ bool wait_gemms(uint64_t* bar, uint32_t& phase, unsigned int* err) {
   const bool ok = tc::mbar_wait_bounded(bar, phase, 1u << 22);
   if (!ok) atomicAdd(err, 1u);
+  const bool all_ok = __syncthreads_or(ok ? 0 : 1) == 0;
+  if (!all_ok) {
+    const bool drained = tc::mbar_wait_bounded(bar, phase, 1u << 26);
+    if (!drained && threadIdx.x == 0) atomicAdd(err, 1u);
+    __syncthreads();
+  }
   phase ^= 1u;
   tc::fence_after_sync();
-  return __syncthreads_or(ok ? 0 : 1) == 0;
+  return all_ok;
 }
 
 __device__ __forceinline__ bool run_gemm(uint32_t tmem_d, const void* a, const void* b, int K, int N, uint64_t* bar,

@@ -18,7 +18,13 @@
 //    (different streams, or different host threads) race on the array.
 //  - The first call on a device resolves the array's device address with
 //    cudaGetSymbolAddress, with that device current; make that first call
-//    before any stream capture.
+//    before any stream capture. The address is kept for the life of the
+//    process: after cudaDeviceReset (which also frees every handle's memory)
+//    the module may load at another address, so this library must not be
+//    used across a device reset.
+//  - Every refusal (null arguments, configuration, boundary kinds, device
+//    ordinal, grid size) is decided on the host before any CUDA call, and
+//    before the state pointers are used.
 //
 // Compiled with -fmad=false like the FP64 stage runner, so the results equal
 // fvh_primitives (and the reference) bit for bit.
@@ -68,6 +74,7 @@ int scratch_address(int device, double** out) {
 
 namespace fvh {
 int configure_handle(fvh_handle* h, const fvh_config* cfg, std::string& msg);
+int check_device_visible(const fvh_config* cfg, std::string& msg);
 }
 
 extern "C" {
@@ -77,12 +84,13 @@ size_t fvh_primitives_noalloc_max_doubles(void) { return kNoAllocScratchDoubles 
 const char* fvh_primitives_noalloc_error(void) { return g_noalloc_error; }
 
 int fvh_primitives_noalloc(const fvh_config* cfg, const double* u, double* w, int fv_average, void* stream) {
-  if (!cfg || !u || !w) return set_error(FVH_ERR_ARG, "null argument");
+  if (!cfg) return set_error(FVH_ERR_ARG, "null configuration");
   fvh_handle h;  // host-side geometry only; no device memory behind it
   std::string msg;
   const int st = fvh::configure_handle(&h, cfg, msg);
   if (st) return set_error(st, msg.c_str());
-  if (h.cfg.device >= kMaxDevices) return set_error(FVH_ERR_CONFIG, "device ordinal too large");
+  if (h.cfg.device < 0 || h.cfg.device >= kMaxDevices)
+    return set_error(FVH_ERR_CONFIG, "device ordinal out of range [0, 64)");
   for (int a = 0; a < 3; ++a)
     for (int side = 0; side < 2; ++side)
       if (h.active[a] && (cfg->bc[a][side] == FVH_BC_DIRICHLET || cfg->bc[a][side] == FVH_BC_DMR_Y0))
@@ -99,6 +107,8 @@ int fvh_primitives_noalloc(const fvh_config* cfg, const double* u, double* w, in
                   need, limit);
     return FVH_ERR_CONFIG;
   }
+  if (!u || !w) return set_error(FVH_ERR_ARG, "null state or output array");
+  if (int sd = fvh::check_device_visible(cfg, msg)) return set_error(sd, msg.c_str());
   cudaError_t e = cudaSetDevice(h.cfg.device);
   if (e != cudaSuccess) return set_error(FVH_ERR_CUDA, cudaGetErrorString(e));
   double* base = nullptr;

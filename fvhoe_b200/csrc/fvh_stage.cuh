@@ -149,6 +149,11 @@ inline int set_cuda_error(fvh_handle* h, const char* what) {
   return FVH_ERR_CUDA;
 }
 
+inline int fail_config(fvh_handle* h, const char* what) {
+  h->err = what;
+  return FVH_ERR_CONFIG;
+}
+
 template <typename Tc>
 inline Phys<Tc> make_phys(const fvh_handle* h) {
   Phys<Tc> ph;
@@ -286,6 +291,8 @@ int primitive_pass(fvh_handle* h, const double* state, int g, Tc* dst, const Red
     out.n[a] = h->n[a] + 2 * ga;
     const bool last = (q == na - 1);
     Tc* o = (last && !fv_average) ? dst : bufs[which];
+    if (o != dst && (size_t)h->nv * (size_t)region_points(out) > h->buf_elems)
+      return fail_config(h, "primitive pass: a sweep box exceeds the scratch buffers");
     launch_centre<Tc, NV>(q == 0, last, src, rsrc, o, out, a, centre_rule(h->p[a]), h->grid, ph, s);
     src = o;
     rsrc = out;
@@ -300,6 +307,8 @@ int primitive_pass(fvh_handle* h, const double* state, int g, Tc* dst, const Red
       out.n[a] = h->n[a] + 2 * g;
       const bool last = (q == na - 1);
       Tc* o = last ? dst : bufs[which];
+      if (o != dst && (size_t)h->nv * (size_t)region_points(out) > h->buf_elems)
+        return fail_config(h, "primitive pass: a sweep box exceeds the scratch buffers");
       launch_transverse<Tc, NV>(last && reduce, (const Tc*)src, rsrc, o, out, a, transverse_rule(h->p[a]), ph, rs,
                                 h->sc, s);
       src = o;

@@ -111,6 +111,12 @@ class Ensemble:
         """n SSP-RK3 steps of every active member (asynchronous)."""
         self._check(self._capi.lib.fvh_ensemble_step(self._e, int(n), self._stream()))
 
+    def set_wait_limit(self, polls: int = 0):
+        """Bound of the grid-barrier waits in polls (0: the default, 2^24); a wait
+        that runs out ends the stage and status() then raises FVH_ERR_TIMEOUT
+        until the next reset."""
+        self._check(self._capi.lib.fvh_ensemble_set_wait_limit(self._e, int(polls)))
+
     def status(self) -> dict:
         n = len(self.members)
         t = (ctypes.c_double * n)()

@@ -9,6 +9,7 @@ all stages of the chosen integrator on the device and returns the step's dt
 (shortened to the next downbeat when `exact`, fvhoe/ode.py:11-22).
 """
 
+import math
 import os
 from abc import ABC, abstractmethod
 from typing import Any, Optional
@@ -107,7 +108,15 @@ class ODE(ABC):
         """(dt, dudt) of one right-hand-side evaluation."""
 
     def take_step(self, target_time: float = None):
+        # a failed update raises from _device_step (FVH_ERR_NONFINITE); a step
+        # that cannot advance the time is refused here, so integrate(T) never
+        # spins on a frozen t (the reference's loop, fvhoe/ode.py:157, would)
         dt = self._device_step(self.integrator, target_time)
+        if not (math.isfinite(dt) and dt > 0.0):
+            raise FloatingPointError(f"step {self.step_count + 1} at t={self.t!r}: dt={dt!r} is not a finite "
+                                     "positive time step")
+        if self.t + dt == self.t:
+            raise FloatingPointError(f"step {self.step_count + 1} at t={self.t!r}: dt={dt!r} does not advance t")
         self.t += dt
         self.timestamps.append(self.t)
         self.step_count += 1

@@ -147,20 +147,38 @@ size_t fvh_scratch_bytes(const fvh_handle* h);
  * evaluation. Replaces EulerSolver.f / hydrodynamics (fvhoe/solver.py:422-454)
  * including revise_fluxes (:653-732) and euler_equation (:734-751).
  * u, dudt: device arrays of nvars * nx * ny * nz doubles. dt_out: host
- * pointer or NULL; when given, the call synchronises the stream. */
+ * pointer or NULL; when given, the call synchronises the stream and returns
+ * FVH_ERR_NONFINITE (with *dt_out written) when dudt holds NaN/Inf values or
+ * dt is not finite or not positive. */
 int fvh_rhs(fvh_handle* h, const double* u, double* dudt, double* dt_out, void* stream);
 
 /* One time step of the chosen integrator, updating u in place. The first
  * stage's dt is shortened to target - t when has_target is set and the target
  * is closer (fvhoe/ode.py:11-22). Replaces ODE.take_step with the stepper of
  * ODE.euler/ssprk2/ssprk3/rk4 (fvhoe/ode.py:183-193, 245-298).
- * dt_out: host pointer or NULL (when given, the stream is synchronised). With
+ * dt_out: host pointer or NULL (when given, the stream is synchronised and
+ * the call returns FVH_ERR_NONFINITE, with *dt_out written, when the step
+ * wrote NaN/Inf values or its dt is not finite or, for a CFL dt, not
+ * positive; fvh_get_stats reports the count either way). With
  * dt_out = NULL the call makes no host synchronisation and can be captured in
  * a CUDA graph after one uncaptured call of the same handle; each replay
  * computes its own dt on the device and reuses the captured t, target and
  * trouble-log mode, so capture steps without a target (or with a fixed one). */
 int fvh_step(fvh_handle* h, double* u, int integrator, double t, int has_target, double target, double* dt_out,
              void* stream);
+
+/* One stage k (0-based) of a step of the chosen integrator, on the caller's
+ * stream: the right-hand-side evaluation of the stage's input and its
+ * Runge-Kutta combination, as one stage of the steppers of fvhoe/ode.py:245-298
+ * (for SSP-RK3, one self.f call of ode.py:274-280 and the sum that follows it).
+ * Stage 0 reads u and fixes the step's dt (CFL, then the target clamp, as in
+ * fvh_step); stage k > 0 reads the handle's stage buffer written by stage k-1;
+ * the last stage writes u in place. Stages of one step must be called in
+ * order, with the same integrator and u (a stage 0 call starts a new step);
+ * the stages of a step equal one fvh_step call bit for bit. dt_out: the step's
+ * dt, as for fvh_step (NULL: no synchronisation). */
+int fvh_stage(fvh_handle* h, double* u, int integrator, int k, double t, int has_target, double target,
+              double* dt_out, void* stream);
 
 /* fvh_step for a state held in page-locked host memory (cudaHostAlloc or
  * cudaHostRegister), as the reference holds u in host NumPy arrays: the call
@@ -194,9 +212,12 @@ int fvh_primitives(fvh_handle* h, const double* u, double* w, int fv_average, vo
  * fvh_primitives_noalloc_max_doubles() doubles per buffer
  * (nvars * prod(n_a + 4 ceil(p_a/2)) over the active axes) are refused with
  * FVH_ERR_CONFIG, and so are Dirichlet and FVH_BC_DMR_Y0 sides, whose
- * ghost values live in a handle. The first call on a device resolves the array's address
- * (make it before any stream capture). All calls share the array: calls whose
- * work overlaps on the GPU race. Errors: fvh_primitives_noalloc_error(). */
+ * ghost values live in a handle. Every refusal is decided on the host before
+ * u or w is used. The first call on a device resolves the array's address
+ * (make it before any stream capture) and keeps it for the life of the
+ * process, so do not use this library across cudaDeviceReset. All calls share
+ * the array: calls whose work overlaps on the GPU race.
+ * Errors: fvh_primitives_noalloc_error(). */
 int fvh_primitives_noalloc(const fvh_config* cfg, const double* u, double* w, int fv_average, void* stream);
 size_t fvh_primitives_noalloc_max_doubles(void);
 const char* fvh_primitives_noalloc_error(void);
@@ -397,6 +418,13 @@ int fvh_ensemble_status(fvh_ensemble* e, double* t, int* steps, int* active, uns
 int fvh_ensemble_configure(fvh_ensemble* e, int variant, int blocks_per_sm, int use_graph);
 int fvh_ensemble_variant_info(fvh_ensemble* e, int variant, int* tx, int* ty, int* max_blocks_per_sm,
                               size_t* smem_bytes);
+/* Bound of the grid-barrier waits between the phases of a stage, in polls of
+ * about 64 ns each (0 restores the default, 2^24 polls). A wait that runs out
+ * raises an abort flag that every block checks at its next barrier, so all
+ * blocks return; fvh_ensemble_status then reports FVH_ERR_TIMEOUT until
+ * fvh_ensemble_reset clears it. Used by tests to show that a stalled stage
+ * ends with a status instead of a hang. */
+int fvh_ensemble_set_wait_limit(fvh_ensemble* e, unsigned int polls);
 /* Times `steps` steps of every variant and block count on the ensemble's own
  * data (restoring states and times after each trial) and keeps the fastest. */
 int fvh_ensemble_autotune(fvh_ensemble* e, int steps, int* variant_out, int* blocks_out, double* ms_per_step,

@@ -2,7 +2,9 @@
 
 Run in a checkout where the reference FVHOE package is importable:
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <FVHOE checkout>
+
+(or set FVHOE_REFERENCE to the checkout instead of passing --reference).
 
 The reference imports matplotlib for plotting only; a placeholder package in
 tests/golden/_mpl_stub stands in for it. Every fixture stores the solver
@@ -323,9 +325,12 @@ def run_case(case, outdir):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("FVHOE_REFERENCE"),
+                    help="the FVHOE checkout to run (default: $FVHOE_REFERENCE)")
     ap.add_argument("--only", default=None)
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("name the FVHOE checkout with --reference or FVHOE_REFERENCE")
     _setup(args.reference)
     _patch_dmr_free_bc()
     cases = build_cases()

@@ -347,3 +347,61 @@ def test_host_state_entry_points_refuse_null_arguments():
 
     assert _capi.lib.fvh_step_host(None, None, 2, 0.0, 0, 0.0, None, None) == _capi.ERR_ARG
     assert _capi.lib.fvh_host_sync(None) == _capi.ERR_ARG
+
+
+def _noalloc_config(**change):
+    from fvhoe_b200 import _capi
+
+    c = _capi.default_config()
+    c.n[0], c.n[1], c.p[0], c.p[1] = 64, 48, 3, 3
+    c.h[0], c.h[1] = 1 / 64, 1 / 48
+    c.device = 0
+    for key, val in change.items():
+        if key == "bc":
+            for a in range(3):
+                c.bc[a][0], c.bc[a][1] = val[a]
+        elif key in ("n", "p"):
+            for a in range(3):
+                getattr(c, key)[a] = val[a]
+        else:
+            setattr(c, key, val)
+    return c
+
+
+@pytest.mark.parametrize(
+    "change, code, message",
+    [
+        (dict(bc=((4, 4), (0, 0), (0, 0))), "ERR_CONFIG", "need a handle"),
+        (dict(bc=((1, 1), (5, 1), (0, 0))), "ERR_CONFIG", "need a handle"),
+        (dict(device=64), "ERR_CONFIG", "device ordinal out of range"),
+        (dict(device=-1), "ERR_CONFIG", "device ordinal out of range"),
+        (dict(n=(1024, 1024, 1), p=(5, 5, 0)), "ERR_CONFIG", "grid too large"),
+        (dict(p=(9, 3, 0)), "ERR_CONFIG", "p must be in [0, 8]"),
+    ],
+)
+def test_noalloc_refusals_are_decided_on_the_host(change, code, message):
+    """Every refusal of the allocation-free conversion comes before any CUDA call
+    and before the state pointers are used, so null pointers are safe here."""
+    from fvhoe_b200 import _capi
+
+    cfg = _noalloc_config(**change)
+    st = _capi.lib.fvh_primitives_noalloc(ctypes.byref(cfg), None, None, 1, None)
+    assert st == getattr(_capi, code)
+    assert message in _capi.lib.fvh_primitives_noalloc_error().decode()
+
+
+def test_noalloc_null_arguments():
+    from fvhoe_b200 import _capi
+
+    assert _capi.lib.fvh_primitives_noalloc(None, None, None, 1, None) == _capi.ERR_ARG
+    assert "null configuration" in _capi.lib.fvh_primitives_noalloc_error().decode()
+    cfg = _noalloc_config()
+    assert _capi.lib.fvh_primitives_noalloc(ctypes.byref(cfg), None, None, 1, None) == _capi.ERR_ARG
+    assert "null state" in _capi.lib.fvh_primitives_noalloc_error().decode()
+
+
+def test_stage_and_wait_limit_refuse_null_handles():
+    from fvhoe_b200 import _capi
+
+    assert _capi.lib.fvh_stage(None, None, 2, 0, 0.0, 0, 0.0, None, None) == _capi.ERR_ARG
+    assert _capi.lib.fvh_ensemble_set_wait_limit(None, 1) == _capi.ERR_ARG

@@ -95,11 +95,19 @@ def test_no_alloc_equals_handle_path_twice(n, p, bc, nvars, fv):
 
 
 def test_no_alloc_refuses_oversized_grids():
+    """Real device arrays of the oversized grid: if the size check ever let the
+    call through, it would fail as a wrong status, not as a stray access."""
+    import torch
+
     from fvhoe_b200 import _capi
 
     limit = _capi.lib.fvh_primitives_noalloc_max_doubles()
     cfg = _config((1024, 1024, 1), (5, 5, 0), "periodic")
     assert 5 * (1024 + 12) ** 2 > limit
-    st = _capi.lib.fvh_primitives_noalloc(ctypes.byref(cfg), ctypes.c_void_p(1), ctypes.c_void_p(1), 1, None)
+    ud = torch.ones((5, 1024, 1024), dtype=torch.float64, device="cuda")
+    wd = torch.empty_like(ud)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    st = _capi.lib.fvh_primitives_noalloc(ctypes.byref(cfg), ctypes.c_void_p(ud.data_ptr()),
+                                          ctypes.c_void_p(wd.data_ptr()), 1, s)
     assert st == _capi.ERR_CONFIG
     assert "too large" in _capi.lib.fvh_primitives_noalloc_error().decode()
