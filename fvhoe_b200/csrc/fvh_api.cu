@@ -8,9 +8,42 @@
 #include <new>
 #include <string>
 
+#include <cudaTypedefs.h>
+
 #include "fvh_handle.h"
+#include "fvh_tma.cuh"
 
 namespace fvh {
+
+bool encode_tensor_map_3d(CUtensorMap* map, const void* base, int elem, int cols, int rows, int nv, int sx, int vs,
+                          int box_cols, int box_rows, int box_vars, const char** why) {
+  // the driver's encoder, reached through the runtime (no link against libcuda)
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      fn = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }();
+  if (!encode) {
+    *why = "cuTensorMapEncodeTiled is not available from the driver";
+    return false;
+  }
+  const cuuint64_t dims[3] = {(cuuint64_t)cols, (cuuint64_t)rows, (cuuint64_t)nv};
+  const cuuint64_t strides[2] = {(cuuint64_t)sx * elem, (cuuint64_t)vs * elem};
+  const cuuint32_t box[3] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows, (cuuint32_t)box_vars};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = encode(map, elem == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                            const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    *why = "cuTensorMapEncodeTiled refused the tile map";
+    return false;
+  }
+  return true;
+}
 
 Profiler::~Profiler() {
   for (auto& p : used_) {
@@ -310,14 +343,20 @@ int allocate(fvh_handle* h) {
   // double-sized even in FP32 mode: the snapshot conversion always runs in FP64
   if ((st = alloc(h, &h->bufA, h->buf_elems * sizeof(double)))) return st;
   if ((st = alloc(h, &h->bufB, h->buf_elems * sizeof(double)))) return st;
-  if ((st = alloc(h, &h->W, nv * (size_t)box(h, h->gW) * el))) return st;
+  // W and W* hold either the generic path's boxes or the fused 2D path's padded rows
+  const bool two_d = h->ndim == 2;
+  const size_t w_elems = std::max((size_t)box(h, h->gW), two_d ? fvh::fused_w_layout(h, h->gW).elems : 0);
+  const size_t ws_elems = std::max((size_t)box(h, 3), two_d ? fvh::fused_w_layout(h, 3).elems : 0);
+  if ((st = alloc(h, &h->W, nv * w_elems * el))) return st;
+  cudaMemset(h->W, 0, nv * w_elems * el);  // padding columns that tile copies read stay zero
   for (int d = 0; d < 3; ++d) {
     if (!h->active[d]) continue;
     const size_t faces = (size_t)ncell / h->n[d] * (h->n[d] + 1);
     if ((st = alloc(h, &h->F[d], nv * faces * el))) return st;
   }
   if (h->cfg.a_posteriori) {
-    if ((st = alloc(h, &h->Ws, nv * (size_t)box(h, 3) * el))) return st;
+    if ((st = alloc(h, &h->Ws, nv * ws_elems * el))) return st;
+    cudaMemset(h->Ws, 0, nv * ws_elems * el);
     if ((st = alloc(h, (void**)&h->Us, nv * (size_t)ncell * sizeof(double)))) return st;
     if ((st = alloc(h, (void**)&h->trouble, (size_t)ncell))) return st;
     if (h->cfg.log_troubles) {
@@ -416,6 +455,9 @@ int read_dt(fvh_handle* h, cudaStream_t s, double* dt_out) {
     return FVH_ERR_CUDA;
   }
   *dt_out = host.dt_step;
+  if (host.timeouts)
+    return fail(h, FVH_ERR_TIMEOUT,
+                std::to_string(host.timeouts) + " tile copies did not complete within their bounded waits");
   if (host.nonfinite)
     return fail(h, FVH_ERR_NONFINITE,
                 "the update wrote " + std::to_string(host.nonfinite) + " non-finite values");

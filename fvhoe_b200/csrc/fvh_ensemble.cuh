@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(256)
     const int li = i - a.prefix[1][q];
     const f2::Geo g = p->g;
     const double dt = a.use_fixed_dt ? a.fixed_dt : p->cfl_h / key_value(p->sc->cfl_key);
-    const f2::V2<const Tc> Wc{(const Tc*)p->W, a.gW, g.ny + 2 * a.gW, (g.nx + 2 * a.gW) * (g.ny + 2 * a.gW)};
+    const f2::V2<const Tc> Wc = f2::make_v2((const Tc*)p->W, g.nx, g.ny, a.gW);
     __syncthreads();
     f2::tile2_fluxes<Tc, P, TX, TY, KC, KF>(Wc, stage_input(p, stage), g, f2::make_v2((Tc*)p->F, g.nx + 1, g.ny, 0),
                                             f2::make_v2((Tc*)p->G, g.nx, g.ny + 1, 0), a.apost ? (Tc*)p->us : nullptr,
@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(256)
       if (!p->active) continue;
       const int li = i - a.prefix[2][q];
       const f2::Geo g = p->g;
-      const f2::V2<const Tc> Wc{(const Tc*)p->W, a.gW, g.ny + 2 * a.gW, (g.nx + 2 * a.gW) * (g.ny + 2 * a.gW)};
+      const f2::V2<const Tc> Wc = f2::make_v2((const Tc*)p->W, g.nx, g.ny, a.gW);
       __syncthreads();
       f2::tile2_detect<Tc, P, TX, TY, KC>((const Tc*)p->us, g, Wc, a.crule, a.trule, a.ph, a.ds, p->sc, p->trouble, nullptr,
                                           nullptr, nullptr, li % p->tiles_y[2], li / p->tiles_y[2], smem_raw);
@@ -228,8 +228,8 @@ __global__ void __launch_bounds__(256)
     st.u = p->u;
     st.acc = p->acc;
     st.next = p->s[stage & 1];
-    const f2::V2<const Tc> Fc{(const Tc*)p->F, 0, g.ny, (g.nx + 1) * g.ny};
-    const f2::V2<const Tc> Gc{(const Tc*)p->G, 0, g.ny + 1, g.nx * (g.ny + 1)};
+    const f2::V2<const Tc> Fc = f2::make_v2((const Tc*)p->F, g.nx + 1, g.ny, 0);
+    const f2::V2<const Tc> Gc = f2::make_v2((const Tc*)p->G, g.nx, g.ny + 1, 0);
     __syncthreads();
     f2::tile2_final<Tc, TX, TY>(st.stage_in, g, Fc, Gc, p->trouble, nullptr, a.apost, 1, a.limiter, a.ph, p->cx, p->cy,
                                 st, p->dt_step, p->sc, li % p->tiles_y[3], li / p->tiles_y[3], smem_raw);

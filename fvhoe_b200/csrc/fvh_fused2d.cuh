@@ -24,6 +24,7 @@
 #pragma once
 
 #include "fvh_kernels.cuh"
+#include "fvh_tma.cuh"
 
 namespace fvh {
 namespace f2 {
@@ -36,14 +37,19 @@ struct Geo {
   const Slabs* slabs;  // Dirichlet ghost values (physical axes), or nullptr
 };
 
-// 2D view of a variable-major array over [-g, nx+g) x [-g, ny'+g).
+// 2D view of a variable-major array over [-g, nx+g) x [-g, ny'+g). Row r of
+// the array holds X index r - g; column c holds Y index c - gy (gy >= g: rows
+// may start with padding, so that Y index 0 and every multiple of 16 bytes
+// from it sit on 16-byte boundaries).
 template <typename T>
 struct V2 {
   T* p;
   int g;   // ghost cells on each side
   int sx;  // row stride (the padded Y extent)
   int vs;  // variable stride
-  __device__ __forceinline__ int at(int x, int y) const { return (x + g) * sx + (y + g); }
+  int gy;  // column of Y index 0
+  __device__ __forceinline__ int at(int x, int y) const { return (x + g) * sx + (y + gy); }
+  __host__ __device__ V2<const T> c() const { return V2<const T>{p, g, sx, vs, gy}; }
 };
 
 template <typename T>
@@ -51,8 +57,25 @@ __host__ __device__ inline V2<T> make_v2(T* p, int nx, int ny, int g) {
   V2<T> v;
   v.p = p;
   v.g = g;
+  v.gy = g;
   v.sx = ny + 2 * g;
   v.vs = (nx + 2 * g) * (ny + 2 * g);
+  return v;
+}
+
+// Rows padded to whole 16-byte vectors: gy and the row stride rounded up to
+// multiples of al elements (16 bytes).
+__host__ __device__ inline int round_up(int n, int al) { return (n + al - 1) / al * al; }
+
+template <typename T>
+__host__ __device__ inline V2<T> make_v2_aligned(T* p, int nx, int ny, int g) {
+  constexpr int al = 16 / (int)sizeof(T);
+  V2<T> v;
+  v.p = p;
+  v.g = g;
+  v.gy = round_up(g, al);
+  v.sx = round_up(v.gy + ny + g, al);
+  v.vs = (nx + 2 * g) * v.sx;
   return v;
 }
 
@@ -482,7 +505,9 @@ __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __res
                                              Tc* __restrict__ ustar, Rule<Tc, KC> c, Rule<Tc, KC> t,
                                              Rule<Tc, KF> lrule, Rule<Tc, KF> rrule, Phys<Tc> ph, double cx,
                                              double cy, double dt, const uint8_t* __restrict__ pred, int muscl,
-                                             int limiter, int bx, int by, unsigned char* smem_raw) {
+                                             int limiter, int bx, int by, unsigned char* smem_raw,
+                                             const CUtensorMap* wmap = nullptr, uint64_t* bar = nullptr,
+                                             unsigned int* tma_err = nullptr) {
   using D = FluxDims<P, TX, TY>;
   constexpr int R = D::R, RC = D::RC, H = D::H, HY = D::HY, VW = VecW<Tc>::value;
   Tc* const S0 = reinterpret_cast<Tc*>(smem_raw);
@@ -497,11 +522,18 @@ __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __res
   Tc* const GY = S2;  // Y face fluxes, TX x GYS
   const int nt = blockDim.x;
   const int x0 = by * TX, y0 = bx * TY;
-  // W tile (W holds gW >= H ghosts; points that no output needs are clamped
-  // into range), VW columns per access where W's rows are 16-byte aligned
-  {
+  // W tile (W holds gW >= H ghosts). With a tensor map: one TMA box copy of
+  // rows x0-H.. and columns y0-HY.. (16-byte aligned: y0, HY and W.gy are
+  // multiples of 16 bytes), rows past the array read as zero and padding
+  // columns as the zeros they were set to; those points feed no output.
+  // Without: per-thread loads, points that no output needs clamped into
+  // range, VW columns per access where W's rows are 16-byte aligned.
+  if (wmap) {
+    tma::stage_box(Ws, wmap, y0 - HY + W.gy, x0 - H + W.g, 0, (uint32_t)(5 * D::WX * D::WYS * sizeof(Tc)), bar,
+                   tma_err);
+  } else {
     constexpr int NG = D::WYS / VW;
-    const bool vec = ((W.g | W.sx | W.vs) & (VW - 1)) == 0 && (reinterpret_cast<uintptr_t>(W.p) & 15) == 0;
+    const bool vec = ((W.gy | W.sx | W.vs) & (VW - 1)) == 0 && (reinterpret_cast<uintptr_t>(W.p) & 15) == 0;
     for (int i = threadIdx.x; i < D::WX * NG; i += nt) {
       const int r = i / NG, cq = (i - r * NG) * VW;
       const int x = min(max(x0 - H + r, -W.g), g.nx + W.g - 1), y = y0 - HY + cq;
@@ -724,8 +756,9 @@ __global__ void __launch_bounds__(256, sizeof(Tc) == 4 ? 4 : 3)
     k2_fluxes(V2<const Tc> W, const double* __restrict__ u, Geo g, V2<Tc> F, V2<Tc> G, Tc* __restrict__ ustar,
               Rule<Tc, KC> c, Rule<Tc, KC> t, Rule<Tc, KF> lrule, Rule<Tc, KF> rrule, Phys<Tc> ph, double cx,
               double cy, Scalars* __restrict__ sc, DtSpec dts, const uint8_t* __restrict__ pred, int muscl,
-              int limiter) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+              int limiter, const __grid_constant__ CUtensorMap wmap) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar;
   // every block derives dt from the reduced CFL key; block (0, 0) publishes it
   const double dt = dts.use_fixed ? dts.fixed_dt : dts.cfl_h / key_value(sc->cfl_key);
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
@@ -737,7 +770,7 @@ __global__ void __launch_bounds__(256, sizeof(Tc) == 4 ? 4 : 3)
     }
   }
   tile2_fluxes<Tc, P, TX, TY, KC, KF>(W, u, g, F, G, ustar, c, t, lrule, rrule, ph, cx, cy, dt, pred, muscl, limiter,
-                                      blockIdx.x, blockIdx.y, smem_raw);
+                                      blockIdx.x, blockIdx.y, smem_raw, &wmap, &bar, &sc->timeouts);
 }
 
 // ---------------------------------------------------------------------------
@@ -745,20 +778,13 @@ __global__ void __launch_bounds__(256, sizeof(Tc) == 4 ? 4 : 3)
 // its 3-cell ring, for the ensemble's persistent phase) and the staged form
 // (W* precomputed over the grid, for the one-problem launches).
 // ---------------------------------------------------------------------------
-// Troubled-cell detection of the tile's cells (fvhoe/slope_limiting.py:87-244)
-// from W* on [x0-3, x0+TX+3) x [y0-3, y0+TY+3) in A (row stride OYS) and W
-// (global, >= 3 ghosts), staged into the free buffer B (BCAP elements).
-template <typename Tc, int TX, int TY, int OYS, int BCAP>
-__device__ __forceinline__ void detect_cells(const Tc* __restrict__ A, Tc* __restrict__ B, const Geo& g,
-                                             const V2<const Tc>& W, const DetectSpec& ds, Scalars* __restrict__ sc,
-                                             uint8_t* __restrict__ trouble, double* __restrict__ log_trouble,
-                                             double* __restrict__ log_nad, double* __restrict__ log_pad, int x0,
+// W on [x0-1, x0+TX+1) x [y0-1, y0+TY+1) into Wt ((TX+2) x (TY+2) per variable)
+// by per-thread loads, clamped into W's ghost range (points past it feed only
+// cells outside the grid), for the 3x3 box extrema of detect_cells.
+template <typename Tc, int TX, int TY>
+__device__ __forceinline__ void stage_w_ring(Tc* __restrict__ Wt, const Geo& g, const V2<const Tc>& W, int x0,
                                              int y0) {
-  constexpr int OX = TX + 6;
-  // stage W on [x0-1, x0+TX+1) x [y0-1, y0+TY+1) in B for the 3x3 box extrema
   constexpr int WX = TX + 2, WY = TY + 2;
-  static_assert(WX * WY * 5 <= BCAP, "W tile must fit in the second buffer");
-  Tc* Wt = B;
   for (int i = threadIdx.x; i < WX * WY; i += blockDim.x) {
     const int r = i / WY, q = i - r * WY;
     const int x = min(x0 - 1 + r, g.nx + W.g - 1), y = min(y0 - 1 + q, g.ny + W.g - 1);
@@ -766,6 +792,20 @@ __device__ __forceinline__ void detect_cells(const Tc* __restrict__ A, Tc* __res
 #pragma unroll
     for (int v = 0; v < 5; ++v) Wt[(v * WX + r) * WY + q] = p[v * W.vs];
   }
+}
+
+// Troubled-cell detection of the tile's cells (fvhoe/slope_limiting.py:87-244)
+// from W* on [x0-3, x0+TX+3) x [y0-3, y0+TY+3) in A (row stride OYS) and W on
+// [x0-1, x0+TX+1) x [y0-1, y0+TY+1) in Wt (row stride WYS, variable stride
+// (TX+2) WYS), both staged by the caller; the first read follows a barrier.
+template <typename Tc, int TX, int TY, int OYS, int WYS>
+__device__ __forceinline__ void detect_cells(const Tc* __restrict__ A, const Tc* __restrict__ Wt, const Geo& g,
+                                             const DetectSpec& ds, Scalars* __restrict__ sc,
+                                             uint8_t* __restrict__ trouble, double* __restrict__ log_trouble,
+                                             double* __restrict__ log_nad, double* __restrict__ log_pad, int x0,
+                                             int y0) {
+  constexpr int OX = TX + 6;
+  constexpr int WX = TX + 2, WY = WYS;
   __syncthreads();
   Tc grange[5], glower[5], gupper[5];
 #pragma unroll
@@ -861,54 +901,85 @@ __device__ __forceinline__ void tile2_detect(const Tc* __restrict__ ustar, Geo g
   Tc* B = A + D::A;
   const int x0 = by * TX, y0 = bx * TY;
   primitives_tile<Tc, P, OX, OY, KC>(ustar, g, x0 - 3, y0 - 3, A, B, c, t, ph);
-  // A now holds W* on [x0-3, x0+TX+3) x [y0-3, y0+TY+3); B is free
-  detect_cells<Tc, TX, TY, D::OYS, D::B>(A, B, g, W, ds, sc, trouble, log_trouble, log_nad, log_pad, x0, y0);
+  // A now holds W* on [x0-3, x0+TX+3) x [y0-3, y0+TY+3); B is free for the W tile
+  static_assert((TX + 2) * (TY + 2) * 5 <= D::B, "W tile must fit in the second buffer");
+  stage_w_ring<Tc, TX, TY>(B, g, W, x0, y0);
+  detect_cells<Tc, TX, TY, D::OYS, TY + 2>(A, B, g, ds, sc, trouble, log_trouble, log_nad, log_pad, x0, y0);
 }
 
 
 // Detection from a precomputed W*: the primitive kernel run on the candidate
 // over the 3-ghost box (Wst) replaces the W* tile that tile2_detect computes
 // on each tile plus its 3-cell ring; the cells and results are the same.
-template <typename Tc, int TX, int TY>
+// Both tiles arrive by TMA box copies whose first column is rounded down to a
+// 16-byte boundary (AL elements): the W* box starts at column y0-4 (Wst.gy is
+// 4, so at array column y0, a multiple of AL) and is read from its second
+// column on; the W box starts at W's column y0-1+gy rounded down, and is read
+// from offset WOFF = (gy(gW) - 1) mod AL, with gW the ghost width of W for
+// degree P with limiting, max(R+1, 2R, 3).
+template <typename Tc, int P, int TX, int TY>
 struct DetectStagedDims {
-  static constexpr int VW = VecW<Tc>::value;
-  static constexpr int OX = TX + 6, OY = TY + 6, OYS = (OY + VW - 1) / VW * VW;
-  static constexpr int A = OX * OYS * 5 + 16;         // W* tile
-  static constexpr int B = (TX + 2) * (TY + 2) * 5 + 16;  // W tile
-  static constexpr int TOTAL = A + B;                 // elements of the compute type
+  static constexpr int AL = 16 / (int)sizeof(Tc);
+  static constexpr int R = (P + 1) / 2;
+  static constexpr int GW = Max<Max<R + 1, 2 * R>::value, 3>::value;
+  static constexpr int GWY = (GW + AL - 1) / AL * AL;  // gy of W
+  static constexpr int WOFF = (GWY - 1) % AL;
+  static constexpr int OX = TX + 6, OYS = (TY + 7 + AL - 1) / AL * AL;      // W* box: columns y0-4 ..
+  static constexpr int WX = TX + 2, WYS = (TY + 2 + WOFF + AL - 1) / AL * AL;  // W box
+  static constexpr int BOXA = OX * OYS * 5, BOXB = WX * WYS * 5;  // elements of the two box copies
+  static constexpr int A = (BOXA + 31) / 32 * 32;  // W* tile, rounded so that the W tile starts 128-byte aligned
+  static constexpr int B = BOXB;                   // W tile
+  static constexpr int TOTAL = A + B;              // elements of the compute type
 };
 
-template <typename Tc, int TX, int TY>
+template <typename Tc, int P, int TX, int TY>
 __device__ __forceinline__ void tile2_detect_staged(V2<const Tc> Wst, Geo g, V2<const Tc> W, DetectSpec ds,
                                                     Scalars* __restrict__ sc, uint8_t* __restrict__ trouble,
                                                     double* __restrict__ log_trouble, double* __restrict__ log_nad,
                                                     double* __restrict__ log_pad, int bx, int by,
-                                                    unsigned char* smem_raw) {
-  using D = DetectStagedDims<Tc, TX, TY>;
+                                                    unsigned char* smem_raw, const CUtensorMap* wsmap,
+                                                    const CUtensorMap* wmap, uint64_t* bars) {
+  using D = DetectStagedDims<Tc, P, TX, TY>;
   Tc* A = reinterpret_cast<Tc*>(smem_raw);
   Tc* B = A + D::A;
   const int x0 = by * TX, y0 = bx * TY;
-  // W* on [x0-3, x0+TX+3) x [y0-3, y0+TY+3), clamped into the 3-ghost box
-  // (points past it feed only cells outside the grid)
-  for (int i = threadIdx.x; i < D::OX * D::OY; i += blockDim.x) {
-    const int r = i / D::OY, q = i - r * D::OY;
-    const int x = min(x0 - 3 + r, g.nx + 2), y = min(y0 - 3 + q, g.ny + 2);
-    const Tc* p = Wst.p + Wst.at(x, y);
-#pragma unroll
-    for (int v = 0; v < 5; ++v) A[(v * D::OX + r) * D::OYS + q] = p[v * Wst.vs];
+  // W* rows x0-3.. (array row x0), columns y0-4.. (array column y0); W rows
+  // x0-1.. (array row x0-1+gW), columns y0-1+gy rounded down to AL
+  const uint32_t bytes_a = (uint32_t)(D::BOXA * sizeof(Tc)), bytes_b = (uint32_t)(D::BOXB * sizeof(Tc));
+  const int wcol = y0 - 1 + D::GWY - D::WOFF;  // the host checks W.gy == GWY
+  if (threadIdx.x == 0) {
+    tma::mbar_init(&bars[0], 1);
+    tma::mbar_init(&bars[1], 1);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
-  // detect_cells stages W and synchronises before the first read of either tile
-  detect_cells<Tc, TX, TY, D::OYS, D::B>(A, B, g, W, ds, sc, trouble, log_trouble, log_nad, log_pad, x0, y0);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    tma::arrive_expect_tx(&bars[0], bytes_a);
+    tma::load_3d(A, wsmap, y0 - 4 + Wst.gy, x0 - 3 + Wst.g, 0, &bars[0]);
+    tma::arrive_expect_tx(&bars[1], bytes_b);
+    tma::load_3d(B, wmap, wcol, x0 - 1 + W.g, 0, &bars[1]);
+  }
+  const bool ok = tma::wait_bounded(&bars[0], 0, tma::kWaitPolls) && tma::wait_bounded(&bars[1], 0, tma::kWaitPolls);
+  if (__syncthreads_or(ok ? 0 : 1)) {
+    // drain both copies before the block reads or leaves its shared memory
+    tma::wait_bounded(&bars[0], 0, tma::kDrainPolls);
+    tma::wait_bounded(&bars[1], 0, tma::kDrainPolls);
+    if (threadIdx.x == 0) atomicAdd(&sc->timeouts, 1u);
+  }
+  detect_cells<Tc, TX, TY, D::OYS, D::WYS>(A + 1, B + D::WOFF, g, ds, sc, trouble, log_trouble, log_nad, log_pad, x0,
+                                           y0);
 }
 
-template <typename Tc, int TX, int TY>
+template <typename Tc, int P, int TX, int TY>
 __global__ void __launch_bounds__(256, 6)
     k2_detect_staged(V2<const Tc> Wst, Geo g, V2<const Tc> W, DetectSpec ds, Scalars* __restrict__ sc,
                      uint8_t* __restrict__ trouble, double* __restrict__ log_trouble, double* __restrict__ log_nad,
-                     double* __restrict__ log_pad) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  tile2_detect_staged<Tc, TX, TY>(Wst, g, W, ds, sc, trouble, log_trouble, log_nad, log_pad, blockIdx.x, blockIdx.y,
-                                  smem_raw);
+                     double* __restrict__ log_pad, const __grid_constant__ CUtensorMap wsmap,
+                     const __grid_constant__ CUtensorMap wmap) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bars[2];
+  tile2_detect_staged<Tc, P, TX, TY>(Wst, g, W, ds, sc, trouble, log_trouble, log_nad, log_pad, blockIdx.x, blockIdx.y,
+                                     smem_raw, &wsmap, &wmap, bars);
 }
 
 // ---------------------------------------------------------------------------

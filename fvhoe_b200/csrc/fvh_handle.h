@@ -75,6 +75,30 @@ struct fvh_handle {
 
 namespace fvh {
 
+// Layout of the fused 2D path's primitive arrays (W with g = gW ghosts, W*
+// with g = 3) on the handle's two active axes X (outer) and Y (inner): rows
+// padded so that Y index 0 and the row stride fall on 16-byte boundaries
+// (f2::make_v2_aligned computes the same numbers on the device side).
+struct WLayout {
+  int g, gy, sx, vs;
+  size_t elems;  // per variable
+};
+
+inline WLayout fused_w_layout(const fvh_handle* h, int g) {
+  int ax[3], na = 0;
+  for (int a = 0; a < 3; ++a)
+    if (h->active[a]) ax[na++] = a;
+  const int nx = na == 2 ? h->n[ax[0]] : 1, ny = na == 2 ? h->n[ax[1]] : 1;
+  const int al = 16 / (int)h->elem;
+  WLayout l;
+  l.g = g;
+  l.gy = (g + al - 1) / al * al;
+  l.sx = (l.gy + ny + g + al - 1) / al * al;
+  l.vs = (nx + 2 * g) * l.sx;
+  l.elems = (size_t)l.vs;
+  return l;
+}
+
 struct StageCall {
   const double* stage_in;  // input state of this stage
   StageSpec spec;          // Runge-Kutta epilogue

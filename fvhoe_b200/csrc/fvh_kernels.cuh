@@ -298,6 +298,7 @@ struct Scalars {
   double dt_step;                         // the step's dt after the target clamp
   unsigned int troubled;                  // troubled cells found this stage
   unsigned int nonfinite;                 // cells whose update is not finite
+  unsigned int timeouts;                  // bounded waits (tile copies) that ran out this step
   // learned-predictor counts, summed over the stages of a step
   unsigned int predicted;                 // cells the network flagged
   unsigned int judged;                    // cells the a-posteriori check flagged

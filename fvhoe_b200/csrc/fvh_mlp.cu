@@ -158,7 +158,8 @@ __device__ __forceinline__ void block_tmem_release(uint32_t tmem_base, uint32_t 
 // ---------------------------------------------------------------------------
 template <typename Tw>
 __global__ void __launch_bounds__(128, 4)
-    k_mlp_predict(const Tw* __restrict__ W, int g, int nx, int ny, int4 vid4, const Scalars* __restrict__ sc,
+    k_mlp_predict(const Tw* __restrict__ W, int g, int gy, int sx, int vs, int nx, int ny, int4 vid4,
+                  const Scalars* __restrict__ sc,
                   const unsigned char* __restrict__ img, const float* __restrict__ params, float thr_logit,
                   uint8_t* __restrict__ pred, unsigned int* __restrict__ err) {
   extern __shared__ __align__(128) unsigned char sm[];
@@ -190,8 +191,6 @@ __global__ void __launch_bounds__(128, 4)
     const double range = key_value(sc->vmax_key[vid[v]]) - key_value(sc->vmin_key[vid[v]]);
     inv_s[v] = (float)(1.0 / ((double)kEps * (range > 0.0 ? range : 1.0)));
   }
-  const int sx = ny + 2 * g;
-  const int vs = (nx + 2 * g) * sx;
   const int ncell = nx * ny;
   const int r = threadIdx.x;
   const uint32_t lane = (uint32_t)(threadIdx.x & ~31) << 16;
@@ -202,7 +201,7 @@ __global__ void __launch_bounds__(128, 4)
     // features straight into the operand tile, one 16-byte row of a core matrix per chunk
     if (valid) {
       const int x = cell / ny, y = cell - (cell / ny) * ny;
-      feature_row<Tw>(W, sx, vs, (x + g) * sx + (y + g), vid, inv_s, [&](int c, uint4 q) {
+      feature_row<Tw>(W, sx, vs, (x + g) * sx + (y + gy), vid, inv_s, [&](int c, uint4 q) {
         *reinterpret_cast<uint4*>(A + tc::kmajor_offset(r, 8 * c, kRows)) = q;
       });
     } else {
@@ -440,7 +439,7 @@ __global__ void k_mlp_pack(const float* __restrict__ p, unsigned char* __restric
 
 // Features and labels of every interior cell from a handle's last stage.
 template <typename Tw>
-__global__ void k_mlp_features(const Tw* __restrict__ W, int g, int nx, int ny, int4 vid4,
+__global__ void k_mlp_features(const Tw* __restrict__ W, int g, int gy, int sx, int vs, int nx, int ny, int4 vid4,
                                const Scalars* __restrict__ sc, const uint8_t* __restrict__ trouble,
                                __nv_bfloat16* __restrict__ X, uint8_t* __restrict__ y) {
   const int vid[4] = {vid4.x, vid4.y, vid4.z, vid4.w};
@@ -450,12 +449,10 @@ __global__ void k_mlp_features(const Tw* __restrict__ W, int g, int nx, int ny, 
     const double range = key_value(sc->vmax_key[vid[v]]) - key_value(sc->vmin_key[vid[v]]);
     inv_s[v] = (float)(1.0 / ((double)kEps * (range > 0.0 ? range : 1.0)));
   }
-  const int sx = ny + 2 * g;
-  const int vs = (nx + 2 * g) * sx;
   for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < nx * ny; cell += gridDim.x * blockDim.x) {
     const int x = cell / ny, yy = cell - (cell / ny) * ny;
     uint4* row = reinterpret_cast<uint4*>(X + (size_t)cell * kInPad);
-    feature_row<Tw>(W, sx, vs, (x + g) * sx + (yy + g), vid, inv_s, [&](int c, uint4 q) { row[c] = q; });
+    feature_row<Tw>(W, sx, vs, (x + g) * sx + (yy + gy), vid, inv_s, [&](int c, uint4 q) { row[c] = q; });
     y[cell] = trouble[cell];
   }
 }
@@ -518,14 +515,17 @@ int mlp_predict_stage(fvh_handle* h, cudaStream_t s) {
   const int4 vid = make_int4(0, 1 + ax[0], 1 + ax[1], 4);
   const int tiles = (nx * ny + kRows - 1) / kRows;
   const int grid = tiles < 148 * 4 ? tiles : 148 * 4;  // 4 CTAs per SM: shared memory and TMEM both allow it
+  const WLayout lay = fused_w_layout(h, h->gW);
   LaunchScope scope(KK_PREDICT, (double)nx * ny * (4 * h->elem + 1), s);
   if (h->elem == sizeof(float)) {
     cudaFuncSetAttribute(k_mlp_predict<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPredictSmem);
-    k_mlp_predict<float><<<grid, kRows, kPredictSmem, s>>>((const float*)h->W, h->gW, nx, ny, vid, h->sc, m->img,
+    k_mlp_predict<float><<<grid, kRows, kPredictSmem, s>>>((const float*)h->W, lay.g, lay.gy, lay.sx, lay.vs, nx, ny,
+                                                          vid, h->sc, m->img,
                                                           m->params, h->pred_thr_logit, h->pred, m->err);
   } else {
     cudaFuncSetAttribute(k_mlp_predict<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPredictSmem);
-    k_mlp_predict<double><<<grid, kRows, kPredictSmem, s>>>((const double*)h->W, h->gW, nx, ny, vid, h->sc, m->img,
+    k_mlp_predict<double><<<grid, kRows, kPredictSmem, s>>>((const double*)h->W, lay.g, lay.gy, lay.sx, lay.vs, nx,
+                                                           ny, vid, h->sc, m->img,
                                                            m->params, h->pred_thr_logit, h->pred, m->err);
   }
   const cudaError_t e = cudaGetLastError();
@@ -641,12 +641,13 @@ int fvh_mlp_features(fvh_handle* h, uint16_t* X, uint8_t* y, void* stream) {
   const int4 vid = make_int4(0, 1 + ax[0], 1 + ax[1], 4);
   cudaStream_t s = (cudaStream_t)stream;
   const int grid = (nx * ny + 255) / 256 < 4096 ? (nx * ny + 255) / 256 : 4096;
+  const WLayout lay = fused_w_layout(h, h->gW);
   if (h->elem == sizeof(float))
-    k_mlp_features<float><<<grid, 256, 0, s>>>((const float*)h->W, h->gW, nx, ny, vid, h->sc, h->trouble,
-                                               reinterpret_cast<__nv_bfloat16*>(X), y);
+    k_mlp_features<float><<<grid, 256, 0, s>>>((const float*)h->W, lay.g, lay.gy, lay.sx, lay.vs, nx, ny, vid, h->sc,
+                                               h->trouble, reinterpret_cast<__nv_bfloat16*>(X), y);
   else
-    k_mlp_features<double><<<grid, 256, 0, s>>>((const double*)h->W, h->gW, nx, ny, vid, h->sc, h->trouble,
-                                                reinterpret_cast<__nv_bfloat16*>(X), y);
+    k_mlp_features<double><<<grid, 256, 0, s>>>((const double*)h->W, lay.g, lay.gy, lay.sx, lay.vs, nx, ny, vid,
+                                                h->sc, h->trouble, reinterpret_cast<__nv_bfloat16*>(X), y);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     h->err = std::string("features: ") + cudaGetErrorString(e);

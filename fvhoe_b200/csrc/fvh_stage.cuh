@@ -628,8 +628,8 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     const int gw = h->gW;
     const dim3 grid((g.ny + 2 * gw + T::PY - 1) / T::PY, (g.nx + 2 * gw + T::PX - 1) / T::PX);
     LaunchScope scope(KK_CENTRE, cells * 5 * (8.0 + sizeof(Tc)), s);
-    kern<<<grid, 256, smem, s>>>(c.stage_in, g, f2::make_v2((Tc*)h->W, g.nx, g.ny, gw), gw, crule, trule, ph, rs,
-                                 h->sc);
+    kern<<<grid, 256, smem, s>>>(c.stage_in, g, f2::make_v2_aligned((Tc*)h->W, g.nx, g.ny, gw), gw, crule, trule, ph,
+                                 rs, h->sc);
   }
   if ((st = set_cuda_error(h, "fused primitives"))) return st;
   // the stage's dt is derived (and published) by the flux kernel
@@ -659,10 +659,16 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     set_smem((const void*)kern, smem);
     const dim3 grid((g.ny + T::FY - 1) / T::FY, (g.nx + T::FX - 1) / T::FX);
     // W in, F and G out; with limiting, the state in and the candidate (compute type) out
+    const f2::V2<const Tc> Wc = f2::make_v2_aligned((const Tc*)h->W, g.nx, g.ny, h->gW);
+    // the W tile of every block arrives by one TMA box copy
+    CUtensorMap wmap;
+    const char* why = nullptr;
+    if (!encode_tensor_map_3d(&wmap, Wc.p, (int)sizeof(Tc), Wc.sx, g.nx + 2 * Wc.g, 5, Wc.sx, Wc.vs, D::WYS, D::WX, 5,
+                              &why))
+      return fail_config(h, why);
     LaunchScope scope(KK_FACE, cells * 5 * (3.0 * sizeof(Tc) + (apost ? 8.0 + sizeof(Tc) : 0.0)), s);
-    f2::V2<const Tc> Wc{(const Tc*)h->W, h->gW, g.ny + 2 * h->gW, (g.nx + 2 * h->gW) * (g.ny + 2 * h->gW)};
     kern<<<grid, 256, smem, s>>>(Wc, c.stage_in, g, F, G, apost ? (Tc*)h->Us : nullptr, crule, trule, lrule, rrule, ph,
-                                 cx, cy, h->sc, dts, pred, 1, cfg.slope_limiter);
+                                 cx, cy, h->sc, dts, pred, 1, cfg.slope_limiter, wmap);
   }
   if ((st = set_cuda_error(h, "fused fluxes"))) return st;
   // 3. W* + detection
@@ -682,7 +688,7 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     ds.log_div = ds.log_mode ? c.log_div : 0.0;
     // W* of the candidate over its 3-ghost box, once per cell: the primitive
     // kernel on u* (no reductions)
-    const f2::V2<Tc> Wst = f2::make_v2((Tc*)h->Ws, g.nx, g.ny, 3);
+    const f2::V2<Tc> Wst = f2::make_v2_aligned((Tc*)h->Ws, g.nx, g.ny, 3);
     {
       using DP = f2::PrimsDims<Tc, P, T::SX, T::SY>;
       const size_t smemp = (size_t)(DP::A + DP::B) * sizeof(Tc);
@@ -693,16 +699,25 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
       kp<<<gp, 256, smemp, s>>>((const Tc*)h->Us, g, Wst, 3, crule, trule, ph, ReduceSpec{}, h->sc);
       if ((st = set_cuda_error(h, "fused candidate primitives"))) return st;
     }
-    using D = f2::DetectStagedDims<Tc, T::DX, T::DY>;
+    using D = f2::DetectStagedDims<Tc, P, T::DX, T::DY>;
     const size_t smem = (size_t)D::TOTAL * sizeof(Tc);
-    auto kern = f2::k2_detect_staged<Tc, T::DX, T::DY>;
+    auto kern = f2::k2_detect_staged<Tc, P, T::DX, T::DY>;
     set_smem((const void*)kern, smem);
     const dim3 grid((g.ny + T::DY - 1) / T::DY, (g.nx + T::DX - 1) / T::DX);
+    const f2::V2<const Tc> Wc = f2::make_v2_aligned((const Tc*)h->W, g.nx, g.ny, h->gW);
+    // both tiles of every block arrive by TMA box copies (column offsets fixed by P)
+    if (Wc.gy != D::GWY || Wst.gy != 4 || Wst.g != 3) return fail_config(h, "detection tile layout mismatch");
+    CUtensorMap wsmap, wmap;
+    const char* why = nullptr;
+    if (!encode_tensor_map_3d(&wsmap, Wst.p, (int)sizeof(Tc), Wst.sx, g.nx + 6, 5, Wst.sx, Wst.vs, D::OYS, D::OX, 5,
+                              &why) ||
+        !encode_tensor_map_3d(&wmap, Wc.p, (int)sizeof(Tc), Wc.sx, g.nx + 2 * Wc.g, 5, Wc.sx, Wc.vs, D::WYS, D::WX, 5,
+                              &why))
+      return fail_config(h, why);
     // W* and W in (compute type), flags out, trouble-log sums in and out
     LaunchScope scope(KK_DETECT, cells * (10.0 * sizeof(Tc) + 1 + (ds.log_mode ? 48.0 : 0.0)), s);
-    f2::V2<const Tc> Wc{(const Tc*)h->W, h->gW, g.ny + 2 * h->gW, (g.nx + 2 * h->gW) * (g.ny + 2 * h->gW)};
-    f2::V2<const Tc> Wsc{Wst.p, Wst.g, Wst.sx, Wst.vs};
-    kern<<<grid, 256, smem, s>>>(Wsc, g, Wc, ds, h->sc, h->trouble, h->logs[0], h->logs[1], h->logs[2]);
+    kern<<<grid, 256, smem, s>>>(Wst.c(), g, Wc, ds, h->sc, h->trouble, h->logs[0], h->logs[1], h->logs[2], wsmap,
+                                 wmap);
     if ((st = set_cuda_error(h, "fused detect"))) return st;
   }
   if (pred && (st = mlp_count_stage(h, s))) return st;
@@ -723,9 +738,7 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
       default: arrays = 1; break;
     }
     LaunchScope scope(KK_FINAL, cells * (5 * 2.0 * sizeof(Tc) + arrays * 40.0 + (apost ? 41.0 : 0.0)), s);
-    f2::V2<const Tc> Fc{F.p, 0, F.sx, F.vs};
-    f2::V2<const Tc> Gc{G.p, 0, G.sx, G.vs};
-    kern<<<grid, 256, smem, s>>>(c.stage_in, g, Fc, Gc, h->trouble, pred, apost ? 1 : 0, 1, cfg.slope_limiter, ph,
+    kern<<<grid, 256, smem, s>>>(c.stage_in, g, F.c(), G.c(), h->trouble, pred, apost ? 1 : 0, 1, cfg.slope_limiter, ph,
                                  cx, cy, c.spec, h->sc);
   }
   return set_cuda_error(h, "fused final");

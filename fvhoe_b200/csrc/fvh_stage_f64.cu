@@ -13,6 +13,7 @@ __global__ void k_reset_scalars(Scalars* sc, int reset_step) {
     sc->troubled = 0u;
     if (reset_step) {
       sc->nonfinite = 0u;
+      sc->timeouts = 0u;
       sc->predicted = 0u;
       sc->judged = 0u;
       sc->missed = 0u;
