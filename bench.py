@@ -420,17 +420,33 @@ def predictor_leg(args, stream, sp):
     v_learned, ms_learned = timed(learned)
     v_learned_k, ms_learned_k = timed(learned_k)
     lk = f"fp32_fused_learned_every{k}"
-    # kernel shares of the predictor form
-    h = learned._handle
-    _capi.check(lib.fvh_profile_enable(h, 1), h)
-    up = ctypes.c_void_p(learned.am("u").data_ptr())
-    _, step = _time_steps(lib, _capi, h, up, sp, stream, 2)
-    K = len(_capi.KERNEL_KINDS)
-    pms = (ctypes.c_double * K)()
-    plaunch = (ctypes.c_uint64 * K)()
-    _capi.check(lib.fvh_profile_read(h, pms, None, plaunch, sp), h)
-    _capi.check(lib.fvh_profile_enable(h, 0), h)
-    shares = {nm: pms[i] / sum(pms) for i, nm in enumerate(_capi.KERNEL_KINDS) if plaunch[i]}
+
+    def kind_ms(s, steps=2):
+        """Per-kind milliseconds per step (CUDA events around each launch)."""
+        h = s._handle
+        _capi.check(lib.fvh_profile_enable(h, 1), h)
+        up = ctypes.c_void_p(s.am("u").data_ptr())
+        _time_steps(lib, _capi, h, up, sp, stream, steps)
+        K = len(_capi.KERNEL_KINDS)
+        pms = (ctypes.c_double * K)()
+        plaunch = (ctypes.c_uint64 * K)()
+        _capi.check(lib.fvh_profile_read(h, pms, None, plaunch, sp), h)
+        _capi.check(lib.fvh_profile_enable(h, 0), h)
+        return {nm: pms[i] / steps for i, nm in enumerate(_capi.KERNEL_KINDS) if plaunch[i]}
+
+    # where the time goes: the predictor saves final-pass revisions and costs
+    # inference plus fallback fluxes in the flux pass
+    km_fused, km_learned, km_k = kind_ms(fused), kind_ms(learned), kind_ms(learned_k)
+    shares = {nm: v / sum(km_learned.values()) for nm, v in km_learned.items()}
+
+    def balance(km):
+        saved = km_fused.get("final", 0.0) - km.get("final", 0.0)
+        flux_added = km.get("face", 0.0) - km_fused.get("face", 0.0)
+        infer = km.get("predict", 0.0)
+        return {"final_pass_saved_ms_per_step": saved, "flux_pass_added_ms_per_step": flux_added,
+                "inference_ms_per_step": infer, "net_ms_per_step": infer + flux_added - saved,
+                "net_without_inference_ms_per_step": flux_added - saved}
+
     errors = net.errors()
     return {
         "config": f"2D Kelvin-Helmholtz {n}x{n}, p={p}, HLLC, SSP-RK3, CFL 0.8, NAD 1e-5 + PAD + SED, periodic",
@@ -453,6 +469,8 @@ def predictor_leg(args, stream, sp):
         "rates_over_l1_run": rates,
         "rates_over_l1_run_every": {lk: rates_k},
         "kernel_shares_learned": shares,
+        "kernel_ms_per_step": {"fp32_fused": km_fused, "fp32_fused_learned": km_learned, lk: km_k},
+        "balance_vs_fp32_fused": {"fp32_fused_learned": balance(km_learned), lk: balance(km_k)},
         "tensor_core_wait_errors": errors,
     }
 

@@ -11,7 +11,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libfvh.so")
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 OK = 0
 ERR_CONFIG = -1
@@ -150,6 +150,8 @@ class FvhPredStats(ctypes.Structure):
         ("troubled", ctypes.c_uint),
         ("missed", ctypes.c_uint),
         ("false_alarm", ctypes.c_uint),
+        ("revised_faces", ctypes.c_uint),
+        ("flux_fallback_faces", ctypes.c_uint),
     ]
 
 

@@ -457,7 +457,8 @@ int read_dt(fvh_handle* h, cudaStream_t s, double* dt_out) {
   *dt_out = host.dt_step;
   if (host.timeouts)
     return fail(h, FVH_ERR_TIMEOUT,
-                std::to_string(host.timeouts) + " tile copies did not complete within their bounded waits");
+                std::to_string(host.timeouts) +
+                    " tile copies were refused (misaligned) or did not complete within their bounded waits");
   if (host.nonfinite)
     return fail(h, FVH_ERR_NONFINITE,
                 "the update wrote " + std::to_string(host.nonfinite) + " non-finite values");
@@ -836,6 +837,8 @@ int fvh_get_pred_stats(fvh_handle* h, fvh_pred_stats* out, void* stream) {
   out->troubled = host.judged;
   out->missed = host.missed;
   out->false_alarm = host.false_alarm;
+  out->revised_faces = host.revised_faces;
+  out->flux_fallback_faces = host.flux_fallback_faces;
   return FVH_OK;
 }
 

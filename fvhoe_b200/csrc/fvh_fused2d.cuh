@@ -223,6 +223,12 @@ __device__ __forceinline__ void stn(double* p, const double* o) {
   }
 }
 
+// Output rows per thread of the sweeps along the strided axis (sweepv's M).
+#ifndef FVH_MROW
+#define FVH_MROW 2
+#endif
+constexpr int MROW = FVH_MROW;
+
 // Elements per shared-memory vector: one 16-byte access (4 floats, 2 doubles).
 template <typename Tc>
 struct VecW {
@@ -239,14 +245,52 @@ struct VecW {
 // group). Row strides IS and variable strides IVS are multiples of VW; outputs
 // past the caller's column count land in the padding of the output rows.
 // IN_LIM bounds the elements the sweep may read from `in`. epi(v, r, q, acc)
-// stores the VW sums.
-template <typename Tc, int VW, int K, int AR, int OFF, int NR, int NG, int IS, int IVS, int IN_LIM, typename Epi>
+// stores the VW sums. M > 1 (AR = 1 only): each thread takes M consecutive
+// output rows and reads each of their M + K - 1 input rows once (a sliding
+// window along the strided axis), every output still summed from tap 0 up.
+template <typename Tc, int VW, int K, int AR, int OFF, int NR, int NG, int IS, int IVS, int IN_LIM, int M = 1,
+          typename Epi>
 __device__ __forceinline__ void sweepv(const Tc* __restrict__ in, const Tc* __restrict__ w, Epi epi) {
   constexpr int S = OFF % VW, B0 = OFF - S;
   constexpr int NW = AR ? (S + 2 * VW - 1) / VW : (S + K + 2 * VW - 2) / VW;
   static_assert(IS % VW == 0 && IVS % VW == 0, "rows and planes must hold whole vectors");
   static_assert(4 * IVS + (NR - 1 + (AR ? K - 1 : 0)) * IS + B0 + VW * (NG - 1) + VW * NW <= IN_LIM,
                 "sweep reads past its shared region");
+  static_assert(M == 1 || AR == 1, "row blocking applies to sweeps along the strided axis");
+  if constexpr (M > 1) {
+    constexpr int NRM = (NR + M - 1) / M;
+    for (int i = threadIdx.x; i < NRM * NG; i += blockDim.x) {
+      const int r0 = (i / NG) * M, q = (i - (i / NG) * NG) * VW;
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const Tc* src = in + v * IVS + B0 + q;
+        Tc acc[M][VW];
+#pragma unroll
+        for (int m = 0; m < M; ++m)
+#pragma unroll
+          for (int j = 0; j < VW; ++j) acc[m][j] = Tc(0);
+#pragma unroll
+        for (int n = 0; n < M + K - 1; ++n) {
+          const int row = min(r0 + n, NR - 1 + K - 1);  // rows past the last output's window feed no output
+          Tc x[VW * NW];
+#pragma unroll
+          for (int u = 0; u < NW; ++u) ldn<VW>(src + row * IS + VW * u, x + VW * u);
+#pragma unroll
+          for (int m = 0; m < M; ++m) {
+            const int k = n - m;
+            if (k >= 0 && k < K) {
+#pragma unroll
+              for (int j = 0; j < VW; ++j) acc[m][j] = acc[m][j] + w[k] * x[S + j];
+            }
+          }
+        }
+#pragma unroll
+        for (int m = 0; m < M; ++m)
+          if (r0 + m < NR) epi(v, r0 + m, q, acc[m]);
+      }
+    }
+    return;
+  }
   for (int i = threadIdx.x; i < NR * NG; i += blockDim.x) {
     const int r = i / NG, q = (i - r * NG) * VW;
 #pragma unroll
@@ -317,7 +361,7 @@ __device__ __forceinline__ void primitives_tile(const Tin* __restrict__ u, const
   }
   __syncthreads();
   // 2. centre sweep along X: B, CX x LYS
-  sweepv<Tc, VW, KC, 1, 0, D::CX, D::LYS / VW, D::LYS, D::LX * D::LYS, D::A>(
+  sweepv<Tc, VW, KC, 1, 0, D::CX, D::LYS / VW, D::LYS, D::LX * D::LYS, D::A, MROW>(
       A, c.w, [&](int v, int r, int q, const Tc* acc) { stn<VW>(B + (v * D::CX + r) * D::LYS + q, acc); });
   __syncthreads();
   // 3. centre sweep along Y, then primitives: A, CX x PYS
@@ -356,7 +400,7 @@ __device__ __forceinline__ void primitives_tile(const Tin* __restrict__ u, const
   }
   __syncthreads();
   // 4. transverse sweep along X: B, OX x PYS
-  sweepv<Tc, VW, KC, 1, 0, OX, D::PYS / VW, D::PYS, D::CX * D::PYS, D::A>(
+  sweepv<Tc, VW, KC, 1, 0, OX, D::PYS / VW, D::PYS, D::CX * D::PYS, D::A, MROW>(
       A, t.w, [&](int v, int r, int q, const Tc* acc) { stn<VW>(B + (v * OX + r) * D::PYS + q, acc); });
   __syncthreads();
   // 5. transverse sweep along Y, into A as an OX x OYS tile
@@ -498,16 +542,18 @@ struct FluxDims {
   static constexpr int LIST = 16 + 2 * ((TX + 1) * TY + TX * (TY + 1));
 };
 
-// FW: faces per thread in the Riemann phases (1, 2 or 4): two in FP32, one in
-// FP64, where two faces' FP64 states would cost a block per SM in registers
-template <typename Tc, int P, int TX, int TY, int KC, int KF, int FW = (sizeof(Tc) == 4 ? 2 : 1)>
+// CHX, CHY: consecutive faces per thread in the two Riemann phases (sliding
+// windows along X and Y); one in FP64, whose states take twice the registers,
+// and fewer along Y for the 9-tap face rules of p = 7, 8 (no register spills)
+template <typename Tc, int P, int TX, int TY, int KC, int KF, int CHX = (sizeof(Tc) == 4 ? 3 : 1),
+          int CHY = (sizeof(Tc) == 4 ? (KF >= 9 ? 2 : 4) : 1)>
 __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __restrict__ u, Geo g, V2<Tc> F, V2<Tc> G,
                                              Tc* __restrict__ ustar, Rule<Tc, KC> c, Rule<Tc, KC> t,
                                              Rule<Tc, KF> lrule, Rule<Tc, KF> rrule, Phys<Tc> ph, double cx,
                                              double cy, double dt, const uint8_t* __restrict__ pred, int muscl,
                                              int limiter, int bx, int by, unsigned char* smem_raw,
                                              const CUtensorMap* wmap = nullptr, uint64_t* bar = nullptr,
-                                             unsigned int* tma_err = nullptr) {
+                                             unsigned int* tma_err = nullptr, unsigned int* fallback_count = nullptr) {
   using D = FluxDims<P, TX, TY>;
   constexpr int R = D::R, RC = D::RC, H = D::H, HY = D::HY, VW = VecW<Tc>::value;
   Tc* const S0 = reinterpret_cast<Tc*>(smem_raw);
@@ -529,8 +575,8 @@ __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __res
   // Without: per-thread loads, points that no output needs clamped into
   // range, VW columns per access where W's rows are 16-byte aligned.
   if (wmap) {
-    tma::stage_box(Ws, wmap, y0 - HY + W.gy, x0 - H + W.g, 0, (uint32_t)(5 * D::WX * D::WYS * sizeof(Tc)), bar,
-                   tma_err);
+    tma::stage_box(Ws, wmap, y0 - HY + W.gy, x0 - H + W.g, 0, (uint32_t)(5 * D::WX * D::WYS * sizeof(Tc)),
+                   (int)sizeof(Tc), bar, tma_err);
   } else {
     constexpr int NG = D::WYS / VW;
     const bool vec = ((W.gy | W.sx | W.vs) & (VW - 1)) == 0 && (reinterpret_cast<uintptr_t>(W.p) & 15) == 0;
@@ -561,38 +607,47 @@ __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __res
       Ws + (H - 1 - R) * D::WYS, c.w,
       [&](int v, int r, int q, const Tc* acc) { stn<VW>(AX + (v * D::AXR + r) * D::AXS + q, acc); });
   // Y faces: AY(r, q) at (x0-RC+r, y0-1-R+q), taps along X
-  sweepv<Tc, VW, KC, 1, HY - 1 - R, D::AYR, D::AYS / VW, D::WYS, D::WX * D::WYS, D::S0 - (H - 2 * RC) * D::WYS>(
+  sweepv<Tc, VW, KC, 1, HY - 1 - R, D::AYR, D::AYS / VW, D::WYS, D::WX * D::WYS, D::S0 - (H - 2 * RC) * D::WYS,
+         MROW>(
       Ws + (H - 2 * RC) * D::WYS, c.w,
       [&](int v, int r, int q, const Tc* acc) { stn<VW>(AY + (v * D::AYR + r) * D::AYS + q, acc); });
   __syncthreads();
   // ---- X faces: face f (x = x0+f) between cells x0+f-1 and x0+f; AX row of
-  // cell x is x - (x0-1-R). FW consecutive columns per thread.
+  // cell x is x - (x0-1-R). Each thread takes one column q and CHX
+  // consecutive faces, sliding along X: per variable, the rows f0 .. f0+CHX+KF-1
+  // are read once into registers and feed all CHX faces (warps run along the
+  // columns, so the scalar reads are conflict-free); every face state is
+  // summed from tap 0 upwards, as a one-face loop sums it.
   {
-    constexpr int NGF = (D::AXC + FW - 1) / FW;
-    for (int i = threadIdx.x; i < D::BXR * NGF; i += nt) {
-      const int f = i / NGF, q = (i - f * NGF) * FW;
-      Tc wl[FW][5], wr[FW][5];
+    constexpr int NCH = (D::BXR + CHX - 1) / CHX;
+    for (int i = threadIdx.x; i < NCH * D::AXC; i += nt) {
+      const int ch = i / D::AXC, q = i - ch * D::AXC;
+      const int f0 = ch * CHX;
+      Tc wl[CHX][5], wr[CHX][5];
 #pragma unroll
       for (int v = 0; v < 5; ++v) {
+        Tc x[CHX + KF];
 #pragma unroll
-        for (int j = 0; j < FW; ++j) wl[j][v] = wr[j][v] = Tc(0);
+        for (int n = 0; n < CHX + KF; ++n) x[n] = AX[(v * D::AXR + min(f0 + n, D::AXR - 1)) * D::AXS + q];
 #pragma unroll
-        for (int k = 0; k <= KF; ++k) {  // row f+k: tap k of the left cell, tap k-1 of the right
-          Tc x[FW];
-          ldn<FW>(AX + (v * D::AXR + f + k) * D::AXS + q, x);
+        for (int j = 0; j < CHX; ++j) {
+          Tc a = Tc(0), b = Tc(0);
 #pragma unroll
-          for (int j = 0; j < FW; ++j) {
-            if (k < KF) wl[j][v] = wl[j][v] + rrule.w[k] * x[j];
-            if (k > 0) wr[j][v] = wr[j][v] + lrule.w[k - 1] * x[j];
+          for (int k = 0; k < KF; ++k) {
+            a = a + rrule.w[k] * x[j + k];
+            b = b + lrule.w[k] * x[j + 1 + k];
           }
+          wl[j][v] = a;
+          wr[j][v] = b;
         }
       }
 #pragma unroll
-      for (int j = 0; j < FW; ++j) {
+      for (int j = 0; j < CHX; ++j) {
+        if (f0 + j >= D::BXR) break;
         Tc fl[5];
         riemann_flux<5>(ph, 5, wl[j], wr[j], g.dx, fl);
 #pragma unroll
-        for (int v = 0; v < 5; ++v) BX[(v * D::BXR + f) * D::AXS + q + j] = fl[v];
+        for (int v = 0; v < 5; ++v) BX[(v * D::BXR + f0 + j) * D::AXS + q] = fl[v];
       }
     }
   }
@@ -611,42 +666,50 @@ __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __res
       });
   __syncthreads();
   // ---- Y faces: face f (y = y0+f) between cells y0+f-1 and y0+f; AY column
-  // of cell y is y - (y0-1-R). FW consecutive faces per thread.
+  // of cell y is y - (y0-1-R). Each thread takes one row r and CHY consecutive
+  // faces, sliding along Y: per variable the columns f0 .. f0+CHY+KF-1 are
+  // read once (in the widest vectors that tile a chunk) and feed all CHY
+  // faces, summed from tap 0 upwards.
   {
-    constexpr int NGF = (TY + 1 + FW - 1) / FW;
-    constexpr int NWF = (KF + 2 * FW - 1) / FW;  // vectors covering columns f .. f+FW+KF-1
-    static_assert(4 * D::AYR * D::AYS + (D::AYR - 1) * D::AYS + (NGF - 1 + NWF) * FW <= D::S2,
+    constexpr int NCH = (TY + 1 + CHY - 1) / CHY;
+    constexpr int LW = CHY % VW == 0 ? VW : (CHY % 2 == 0 ? 2 : 1);  // load width
+    constexpr int NWY = (CHY + KF + LW - 1) / LW;  // loads covering columns f0 .. f0+CHY+KF-1
+    static_assert(D::AYS % VW == 0 && D::BYS % VW == 0, "rows must hold whole vectors");
+    static_assert(5 * D::AYR * D::AYS + (NCH - 1) * CHY + NWY * LW - D::AYS <= D::S2,
                   "Y-face reads past their shared region");
-    for (int i = threadIdx.x; i < D::BYR * NGF; i += nt) {
-      const int r = i / NGF, f = (i - r * NGF) * FW;
-      Tc wl[FW][5], wr[FW][5];
+    static_assert((NCH - 1) * CHY + CHY <= D::BYS, "Y-face chunks must fit the padded rows");
+    for (int i = threadIdx.x; i < D::BYR * NCH; i += nt) {
+      const int r = i / NCH, f0 = (i - r * NCH) * CHY;
+      Tc wl[CHY][5], wr[CHY][5];
 #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        Tc x[NWF * FW];
+        Tc x[NWY * LW];
 #pragma unroll
-        for (int n = 0; n < NWF; ++n) ldn<FW>(AY + (v * D::AYR + r) * D::AYS + f + n * FW, x + n * FW);
+        for (int n = 0; n < NWY; ++n) ldn<LW>(AY + (v * D::AYR + r) * D::AYS + f0 + n * LW, x + n * LW);
 #pragma unroll
-        for (int j = 0; j < FW; ++j) wl[j][v] = wr[j][v] = Tc(0);
+        for (int j = 0; j < CHY; ++j) {
+          Tc a = Tc(0), b = Tc(0);
 #pragma unroll
-        for (int k = 0; k < KF; ++k)
-#pragma unroll
-          for (int j = 0; j < FW; ++j) {
-            wl[j][v] = wl[j][v] + rrule.w[k] * x[j + k];
-            wr[j][v] = wr[j][v] + lrule.w[k] * x[j + 1 + k];
+          for (int k = 0; k < KF; ++k) {
+            a = a + rrule.w[k] * x[j + k];
+            b = b + lrule.w[k] * x[j + 1 + k];
           }
+          wl[j][v] = a;
+          wr[j][v] = b;
+        }
       }
 #pragma unroll
-      for (int j = 0; j < FW; ++j) {
+      for (int j = 0; j < CHY; ++j) {
         Tc fl[5];
         riemann_flux<5>(ph, 5, wl[j], wr[j], g.dy, fl);
 #pragma unroll
-        for (int v = 0; v < 5; ++v) BY[(v * D::BYR + r) * D::BYS + f + j] = fl[v];
+        for (int v = 0; v < 5; ++v) BY[(v * D::BYR + r) * D::BYS + f0 + j] = fl[v];
       }
     }
   }
   __syncthreads();
   // Y face fluxes: transverse sweep along X -> GY and G (owned faces)
-  sweepv<Tc, VW, KC, 1, 0, TX, D::GYS / VW, D::BYS, D::BYR * D::BYS, D::S0>(
+  sweepv<Tc, VW, KC, 1, 0, TX, D::GYS / VW, D::BYS, D::BYR * D::BYS, D::S0, MROW>(
       BY, t.w, [&](int v, int r, int f, const Tc* acc) {
         stn<VW>(GY + (v * TX + r) * D::GYS + f, acc);
         const int x = x0 + r;
@@ -723,6 +786,7 @@ __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __res
   }
   __syncthreads();
   const int nxf = nface[0], nyf = nface[1];
+  if (fallback_count && threadIdx.x == 0) atomicAdd(fallback_count, (unsigned int)(nxf + nyf));
   for (int k = threadIdx.x; k < nxf; k += nt) {
     const int i = xlist[k];
     const int f = i / TY, q = i - f * TY;
@@ -758,7 +822,7 @@ __global__ void __launch_bounds__(256, sizeof(Tc) == 4 ? 4 : 3)
               double cy, Scalars* __restrict__ sc, DtSpec dts, const uint8_t* __restrict__ pred, int muscl,
               int limiter, const __grid_constant__ CUtensorMap wmap) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(8) uint64_t bar;  // before the dynamic block: the tiles start at align128(smem_raw)
   // every block derives dt from the reduced CFL key; block (0, 0) publishes it
   const double dt = dts.use_fixed ? dts.fixed_dt : dts.cfl_h / key_value(sc->cfl_key);
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
@@ -770,7 +834,8 @@ __global__ void __launch_bounds__(256, sizeof(Tc) == 4 ? 4 : 3)
     }
   }
   tile2_fluxes<Tc, P, TX, TY, KC, KF>(W, u, g, F, G, ustar, c, t, lrule, rrule, ph, cx, cy, dt, pred, muscl, limiter,
-                                      blockIdx.x, blockIdx.y, smem_raw, &wmap, &bar, &sc->timeouts);
+                                      blockIdx.x, blockIdx.y, tma::align128(smem_raw), &wmap, &bar, &sc->timeouts,
+                                      &sc->flux_fallback_faces);
 }
 
 // ---------------------------------------------------------------------------
@@ -953,12 +1018,20 @@ __device__ __forceinline__ void tile2_detect_staged(V2<const Tc> Wst, Geo g, V2<
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
+  int refused = 0;
   if (threadIdx.x == 0) {
-    tma::arrive_expect_tx(&bars[0], bytes_a);
-    tma::load_3d(A, wsmap, y0 - 4 + Wst.gy, x0 - 3 + Wst.g, 0, &bars[0]);
-    tma::arrive_expect_tx(&bars[1], bytes_b);
-    tma::load_3d(B, wmap, wcol, x0 - 1 + W.g, 0, &bars[1]);
+    const int acol = y0 - 4 + Wst.gy;
+    if (tma::copy_aligned(A, acol, (int)sizeof(Tc)) && tma::copy_aligned(B, wcol, (int)sizeof(Tc))) {
+      tma::arrive_expect_tx(&bars[0], bytes_a);
+      tma::load_3d(A, wsmap, acol, x0 - 3 + Wst.g, 0, &bars[0]);
+      tma::arrive_expect_tx(&bars[1], bytes_b);
+      tma::load_3d(B, wmap, wcol, x0 - 1 + W.g, 0, &bars[1]);
+    } else {
+      refused = 1;
+      atomicAdd(&sc->timeouts, 1u);
+    }
   }
+  if (__syncthreads_or(refused)) return;  // nothing was copied: the host reports the error
   const bool ok = tma::wait_bounded(&bars[0], 0, tma::kWaitPolls) && tma::wait_bounded(&bars[1], 0, tma::kWaitPolls);
   if (__syncthreads_or(ok ? 0 : 1)) {
     // drain both copies before the block reads or leaves its shared memory
@@ -977,9 +1050,9 @@ __global__ void __launch_bounds__(256, 6)
                      double* __restrict__ log_pad, const __grid_constant__ CUtensorMap wsmap,
                      const __grid_constant__ CUtensorMap wmap) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ __align__(8) uint64_t bars[2];  // before the dynamic block: the tiles start at align128(smem_raw)
   tile2_detect_staged<Tc, P, TX, TY>(Wst, g, W, ds, sc, trouble, log_trouble, log_nad, log_pad, blockIdx.x, blockIdx.y,
-                                     smem_raw, &wsmap, &wmap, bars);
+                                     tma::align128(smem_raw), &wsmap, &wmap, bars);
 }
 
 // ---------------------------------------------------------------------------
@@ -1202,6 +1275,7 @@ __device__ __forceinline__ void tile2_final(const double* __restrict__ stage_in,
     __syncthreads();
     // X faces
     const int nx_faces = nface[0], ny_faces = nface[1];
+    if (threadIdx.x == 0) atomicAdd(&sc->revised_faces, (unsigned int)(nx_faces + ny_faces));
     for (int k = threadIdx.x; k < nx_faces; k += nt) {
       const int i = xlist[k];
       const int f = i / TY, q = i - f * TY;

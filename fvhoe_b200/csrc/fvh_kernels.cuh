@@ -298,12 +298,17 @@ struct Scalars {
   double dt_step;                         // the step's dt after the target clamp
   unsigned int troubled;                  // troubled cells found this stage
   unsigned int nonfinite;                 // cells whose update is not finite
-  unsigned int timeouts;                  // bounded waits (tile copies) that ran out this step
+  unsigned int timeouts;                  // tile copies refused (misaligned) or whose bounded wait ran out, this step
   // learned-predictor counts, summed over the stages of a step
   unsigned int predicted;                 // cells the network flagged
   unsigned int judged;                    // cells the a-posteriori check flagged
   unsigned int missed;                    // judged, not predicted
   unsigned int false_alarm;               // predicted, not judged
+  // faces whose flux the fused path revised, summed over the stages of a step:
+  // by the final pass (troubled cells; with a predictor, only the misses) and
+  // by the flux pass (faces of predicted cells)
+  unsigned int revised_faces;
+  unsigned int flux_fallback_faces;
 };
 
 // Reduction request for the last transverse sweep of the primitive pass.

@@ -654,7 +654,8 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
   // 2. fluxes (+ candidate)
   {
     using D = f2::FluxDims<P, T::FX, T::FY>;
-    const size_t smem = (size_t)D::TOTAL * sizeof(Tc) + (pred ? D::LIST : 0);
+    // 128 spare bytes: the kernel starts its tiles at the first 128-byte boundary (TMA destination)
+    const size_t smem = (size_t)D::TOTAL * sizeof(Tc) + (pred ? D::LIST : 0) + 128;
     auto kern = f2::k2_fluxes<Tc, P, T::FX, T::FY, KC, KF>;
     set_smem((const void*)kern, smem);
     const dim3 grid((g.ny + T::FY - 1) / T::FY, (g.nx + T::FX - 1) / T::FX);
@@ -700,7 +701,7 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
       if ((st = set_cuda_error(h, "fused candidate primitives"))) return st;
     }
     using D = f2::DetectStagedDims<Tc, P, T::DX, T::DY>;
-    const size_t smem = (size_t)D::TOTAL * sizeof(Tc);
+    const size_t smem = (size_t)D::TOTAL * sizeof(Tc) + 128;  // + the alignment slack of the TMA destination
     auto kern = f2::k2_detect_staged<Tc, P, T::DX, T::DY>;
     set_smem((const void*)kern, smem);
     const dim3 grid((g.ny + T::DY - 1) / T::DY, (g.nx + T::DX - 1) / T::DX);

@@ -18,6 +18,8 @@ __global__ void k_reset_scalars(Scalars* sc, int reset_step) {
       sc->judged = 0u;
       sc->missed = 0u;
       sc->false_alarm = 0u;
+      sc->revised_faces = 0u;
+      sc->flux_fallback_faces = 0u;
     }
   }
   for (int v = t; v < kMaxVars; v += blockDim.x) {

@@ -11,7 +11,13 @@
 //    multiple of 16 bytes (nothing checks this before the copy runs, so every
 //    caller derives it from 16-byte aligned quantities only);
 //  - a load may start at or run past the array's end on the outer axes: those
-//    elements read as zero.
+//    elements read as zero;
+//  - the shared-memory destination is 128-byte aligned: kernels round their
+//    dynamic shared memory up to it at run time (align128), since static
+//    shared variables placed before it (their mbarriers) shift its start.
+// Each copy checks the destination's and the inner coordinate's alignment
+// before it is issued; a copy that fails the check is not issued, counts into
+// an error word and is not waited for.
 // Waits are bounded (2^20 polls): a wait that runs out counts into an error
 // word, then the block waits again (2^22 polls) for the copy it issued, so that the copy does
 // not land in shared memory after the block has moved on or exited.
@@ -66,21 +72,40 @@ __device__ __forceinline__ void load_3d(void* dst, const CUtensorMap* map, int c
       : "memory");
 }
 
+// The first 128-byte boundary at or after p (dynamic shared memory requests
+// carry 128 spare bytes for it).
+__device__ __forceinline__ unsigned char* align128(unsigned char* p) {
+  return p + ((128u - (smem_u32(p) & 127u)) & 127u);
+}
+
+// Whether a box copy to dst starting at inner coordinate c0 (elements of
+// elem bytes) meets the alignment rules above.
+__device__ __forceinline__ bool copy_aligned(const void* dst, int c0, int elem) {
+  return (smem_u32(dst) & 127u) == 0 && ((long long)c0 * elem) % 16 == 0;
+}
+
 // Whole block: stages the box at (c0, c1, c2) of map into dst (bytes = the
 // box's size) through bar, which this call initialises (one use per barrier
-// and kernel). Returns false in every thread when the wait ran out (the
-// error word is raised once per block).
+// and kernel). Returns false in every thread when the copy was refused for
+// its alignment or its wait ran out (the error word is raised once per block).
 __device__ __forceinline__ bool stage_box(void* dst, const CUtensorMap* map, int c0, int c1, int c2, uint32_t bytes,
-                                          uint64_t* bar, unsigned int* err) {
+                                          int elem, uint64_t* bar, unsigned int* err) {
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
+  int refused = 0;
   if (threadIdx.x == 0) {
-    arrive_expect_tx(bar, bytes);
-    load_3d(dst, map, c0, c1, c2, bar);
+    if (copy_aligned(dst, c0, elem)) {
+      arrive_expect_tx(bar, bytes);
+      load_3d(dst, map, c0, c1, c2, bar);
+    } else {
+      refused = 1;
+      atomicAdd(err, 1u);
+    }
   }
+  if (__syncthreads_or(refused)) return false;
   const bool ok = wait_bounded(bar, 0, kWaitPolls);
   const bool all_ok = __syncthreads_or(ok ? 0 : 1) == 0;
   if (!all_ok) {

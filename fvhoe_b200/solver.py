@@ -404,8 +404,8 @@ class EulerSolver(ODE):
         st = self._capi.FvhPredStats()
         self._capi.check(self._capi.lib.fvh_get_pred_stats(self._handle, ctypes.byref(st), self._stream()),
                          self._handle)
-        for k in ("predicted", "troubled", "missed", "false_alarm"):
-            self.pred_totals[k] += int(getattr(st, k))
+        for k in ("predicted", "troubled", "missed", "false_alarm", "revised_faces", "flux_fallback_faces"):
+            self.pred_totals[k] = self.pred_totals.get(k, 0) + int(getattr(st, k))
         self.pred_totals["cell_stages"] += stages * int(np.prod(self.n))
 
     def predictor_rates(self) -> dict:

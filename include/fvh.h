@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define FVH_ABI_VERSION 2
+#define FVH_ABI_VERSION 3
 
 /* status codes */
 #define FVH_OK 0
@@ -358,12 +358,18 @@ int fvh_set_predictor(fvh_handle* h, fvh_mlp* m, float threshold);
  * has no predictor). */
 int fvh_set_predictor_interval(fvh_handle* h, int stages);
 
-/* Predictor counts of the last step, summed over its stages. */
+/* Predictor counts of the last step, summed over its stages. The two face
+ * counts are kept by the fused 2D path with or without a predictor: faces
+ * whose flux the final pass revised (the faces of troubled cells; with a
+ * predictor, those of the cells it missed) and faces that took the fallback
+ * flux in the flux pass (those of predicted cells). */
 typedef struct fvh_pred_stats {
   unsigned int predicted;   /* cells the network flagged */
   unsigned int troubled;    /* cells the a-posteriori check flagged */
   unsigned int missed;      /* troubled, not predicted */
   unsigned int false_alarm; /* predicted, not troubled */
+  unsigned int revised_faces;       /* faces revised by the final pass */
+  unsigned int flux_fallback_faces; /* faces given the fallback flux by the flux pass */
 } fvh_pred_stats;
 
 /* Synchronises the stream. */

@@ -8,8 +8,10 @@
   oracle's stage with the fallback applied on (troubled | predicted) cells,
   with the a-posteriori flags unchanged;
 * training: the network trained by the project's kernels on KH / four-quadrant
-  runs predicts held-out flags far better than the untrained network, and the
-  final pass then revises only the missed cells.
+  runs predicts held-out flags far better than the untrained network, and,
+  against the same run without a predictor, the final pass (the revision
+  sweep) revises far fewer faces: the faces of predicted cells take their
+  fallback flux in the flux pass instead.
 """
 
 import os
@@ -190,6 +192,27 @@ def test_trained_predictor_gains_over_untrained():
     print("attached", r)
     assert r["missed"] < 0.2 * r["troubled"]
     assert net.errors() == 0
+    # against the method without the predictor, on the same run: the final
+    # pass (the revision sweep) revises far fewer faces, because the faces of
+    # predicted cells took their fallback flux in the flux pass already
+    import ctypes
+
+    from fvhoe_b200 import _capi
+
+    plain = _kh_solver(128, 9)
+    plain.integrator = "ssprk3"
+    revised_plain = 0
+    for _ in range(10):
+        plain.take_step()
+        st = _capi.FvhPredStats()
+        _capi.check(_capi.lib.fvh_get_pred_stats(plain._handle, ctypes.byref(st), plain._stream()), plain._handle)
+        revised_plain += st.revised_faces
+        assert st.flux_fallback_faces == 0
+    print("final-pass revisions: plain", revised_plain, "with the predictor", r["revised_faces"],
+          "flux-pass fallback faces", r["flux_fallback_faces"])
+    assert revised_plain > 0
+    assert r["revised_faces"] < 0.3 * revised_plain
+    assert r["flux_fallback_faces"] > 0.5 * revised_plain
 
 
 @pytest.mark.parametrize("every,launches", [(1, 6), (2, 3), (3, 2)])
