@@ -19,6 +19,7 @@
 #include <string>
 
 #include "fvh_fused2d.cuh"
+#include "fvh_fused3d.cuh"
 #include "fvh_handle.h"
 #include "fvh_profile.h"
 
@@ -406,6 +407,56 @@ void launch_detect(const fvh_handle* h, const View<const Tc>& w, const View<cons
 }
 
 // ---------------------------------------------------------------------------
+// fused 3D primitive pass (fvh_fused3d.cuh): three active axes, five
+// variables, the same degree p <= 5 on every axis, no Dirichlet sides; the
+// generic path's six sweeps in one tiled launch, bit for bit the same W
+// ---------------------------------------------------------------------------
+inline bool fused3d_prims_eligible(const fvh_handle* h) {
+  return h->cfg.kernel_path != FVH_PATH_GENERIC && h->ndim == 3 && h->nv == 5 && !h->grid.slabs &&
+         h->p[0] == h->p[1] && h->p[1] == h->p[2] && h->p[0] <= 5;
+}
+
+template <typename Tc>
+struct Fused3Tiles;
+template <>
+struct Fused3Tiles<float> {
+  static constexpr int OX = 8, OY = 8, OZ = 16;
+};
+template <>
+struct Fused3Tiles<double> {
+  static constexpr int OX = 8, OY = 4, OZ = 16;
+};
+
+template <typename Tc, int P, bool REDUCE>
+int prims3d_p(fvh_handle* h, const double* state, int g, Tc* dst, const ReduceSpec& rs, cudaStream_t s) {
+  using T = Fused3Tiles<Tc>;
+  constexpr int KC = 2 * (P / 2) + 1;
+  using D = f3::Prims3Dims<Tc, P, T::OX, T::OY, T::OZ>;
+  const size_t smem = (size_t)D::TOTAL * sizeof(Tc);
+  auto kern = f3::k3_primitives<Tc, P, T::OX, T::OY, T::OZ, KC, REDUCE, double>;
+  cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const Region rW = padded_region(h, g);
+  const dim3 grid((rW.n[2] + T::OZ - 1) / T::OZ, (rW.n[1] + T::OY - 1) / T::OY, (rW.n[0] + T::OX - 1) / T::OX);
+  const double pts = (double)region_points(rW);
+  LaunchScope scope(KK_CENTRE, (double)h->n[0] * h->n[1] * h->n[2] * 5 * 8.0 + pts * 5 * sizeof(Tc), s);
+  kern<<<grid, 256, smem, s>>>(state, h->grid, make_view(dst, rW), g, device_rule<Tc, KC>(centre_rule(P)),
+                               device_rule<Tc, KC>(transverse_rule(P)), make_phys<Tc>(h), rs, h->sc);
+  return set_cuda_error(h, "fused 3D primitives");
+}
+
+template <typename Tc, bool REDUCE>
+int prims3d(fvh_handle* h, const double* state, int g, Tc* dst, const ReduceSpec& rs, cudaStream_t s) {
+  switch (h->p[0]) {
+    case 0: return prims3d_p<Tc, 0, REDUCE>(h, state, g, dst, rs, s);
+    case 1: return prims3d_p<Tc, 1, REDUCE>(h, state, g, dst, rs, s);
+    case 2: return prims3d_p<Tc, 2, REDUCE>(h, state, g, dst, rs, s);
+    case 3: return prims3d_p<Tc, 3, REDUCE>(h, state, g, dst, rs, s);
+    case 4: return prims3d_p<Tc, 4, REDUCE>(h, state, g, dst, rs, s);
+    default: return prims3d_p<Tc, 5, REDUCE>(h, state, g, dst, rs, s);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // one stage
 // ---------------------------------------------------------------------------
 template <typename Tc, int NV>
@@ -426,7 +477,12 @@ int run_stage_t(fvh_handle* h, const StageCall& c, cudaStream_t s) {
   rs.ext_box = padded_region(h, 3);
   rs.ndim = (double)h->ndim;
   const Region rW = padded_region(h, h->gW);
-  if ((st = primitive_pass<Tc, NV>(h, c.stage_in, h->gW, (Tc*)h->W, rs, true, true, s))) return st;
+  const bool fused3 = fused3d_prims_eligible(h);
+  if (fused3) {
+    if ((st = prims3d<Tc, true>(h, c.stage_in, h->gW, (Tc*)h->W, rs, s))) return st;
+  } else if ((st = primitive_pass<Tc, NV>(h, c.stage_in, h->gW, (Tc*)h->W, rs, true, true, s))) {
+    return st;
+  }
   // 2. dt
   {
     LaunchScope scope(KK_SMALL, 0.0, s);
@@ -457,7 +513,11 @@ int run_stage_t(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     }
     if ((st = set_cuda_error(h, "candidate"))) return st;
     ReduceSpec none{};
-    if ((st = primitive_pass<Tc, NV>(h, h->Us, 3, (Tc*)h->Ws, none, false, true, s))) return st;
+    if (fused3) {
+      if ((st = prims3d<Tc, false>(h, h->Us, 3, (Tc*)h->Ws, none, s))) return st;
+    } else if ((st = primitive_pass<Tc, NV>(h, h->Us, 3, (Tc*)h->Ws, none, false, true, s))) {
+      return st;
+    }
     DetectSpec ds{};
     ds.nad_global = cfg.nad_global;
     ds.nad_relative = cfg.nad_relative;
