@@ -407,9 +407,10 @@ void launch_detect(const fvh_handle* h, const View<const Tc>& w, const View<cons
 }
 
 // ---------------------------------------------------------------------------
-// fused 3D primitive pass (fvh_fused3d.cuh): three active axes, five
-// variables, the same degree p <= 5 on every axis, no Dirichlet sides; the
-// generic path's six sweeps in one tiled launch, bit for bit the same W
+// fused 3D passes (fvh_fused3d.cuh): three active axes, five variables, the
+// same degree p <= 5 on every axis, no Dirichlet sides; the generic path's six
+// sweeps of a primitive pass in one tiled launch, and its four sweeps and face
+// solve of a direction's flux pass in another, bit for bit the same results
 // ---------------------------------------------------------------------------
 inline bool fused3d_prims_eligible(const fvh_handle* h) {
   return h->cfg.kernel_path != FVH_PATH_GENERIC && h->ndim == 3 && h->nv == 5 && !h->grid.slabs &&
@@ -456,6 +457,45 @@ int prims3d(fvh_handle* h, const double* state, int g, Tc* dst, const ReduceSpec
   }
 }
 
+template <typename Tc, int P, int D>
+int flux3d_pd(fvh_handle* h, Tc* Fd, cudaStream_t s) {
+  using T = Fused3Tiles<Tc>;
+  constexpr int R = (P + 1) / 2, KC = 2 * (P / 2) + 1, KF = 2 * R + 1;
+  using Dm = f3::Flux3Dims<Tc, P, D, T::OX, T::OY, T::OZ>;
+  const size_t smem = (size_t)Dm::TOTAL * sizeof(Tc);
+  auto kern = f3::k3_fluxes<Tc, P, D, T::OX, T::OY, T::OZ, KC, KF>;
+  cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const Region rf = face_region(h, D);
+  const dim3 grid((rf.n[2] + T::OZ - 1) / T::OZ, (rf.n[1] + T::OY - 1) / T::OY, (rf.n[0] + T::OX - 1) / T::OX);
+  const double cells = (double)h->n[0] * h->n[1] * h->n[2];
+  LaunchScope scope(KK_FACE, cells * 5 * sizeof(Tc) + (double)region_points(rf) * 5 * sizeof(Tc), s);
+  kern<<<grid, 256, smem, s>>>(make_view((const Tc*)h->W, padded_region(h, h->gW)), h->gW, h->grid, make_view(Fd, rf),
+                               device_rule<Tc, KC>(centre_rule(P)), device_rule<Tc, KC>(transverse_rule(P)),
+                               device_rule<Tc, KF>(left_face_rule(P)), device_rule<Tc, KF>(right_face_rule(P)),
+                               make_phys<Tc>(h));
+  return set_cuda_error(h, "fused 3D fluxes");
+}
+
+template <typename Tc, int P>
+int flux3d_p(fvh_handle* h, int d, Tc* Fd, cudaStream_t s) {
+  if (d == 0) return flux3d_pd<Tc, P, 0>(h, Fd, s);
+  if (d == 1) return flux3d_pd<Tc, P, 1>(h, Fd, s);
+  return flux3d_pd<Tc, P, 2>(h, Fd, s);
+}
+
+// High-order face fluxes along d of a fused-3D-eligible handle from W.
+template <typename Tc>
+int flux3d(fvh_handle* h, int d, Tc* Fd, cudaStream_t s) {
+  switch (h->p[0]) {
+    case 0: return flux3d_p<Tc, 0>(h, d, Fd, s);
+    case 1: return flux3d_p<Tc, 1>(h, d, Fd, s);
+    case 2: return flux3d_p<Tc, 2>(h, d, Fd, s);
+    case 3: return flux3d_p<Tc, 3>(h, d, Fd, s);
+    case 4: return flux3d_p<Tc, 4>(h, d, Fd, s);
+    default: return flux3d_p<Tc, 5>(h, d, Fd, s);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // one stage
 // ---------------------------------------------------------------------------
@@ -493,7 +533,11 @@ int run_stage_t(fvh_handle* h, const StageCall& c, cudaStream_t s) {
   FluxSet<Tc> fs{};
   for (int d = 0; d < 3; ++d) {
     if (!h->active[d]) continue;
-    if ((st = flux_pass<Tc, NV>(h, (const Tc*)h->W, rW, d, (Tc*)h->F[d], s))) return st;
+    if (fused3) {
+      if ((st = flux3d<Tc>(h, d, (Tc*)h->F[d], s))) return st;
+    } else if ((st = flux_pass<Tc, NV>(h, (const Tc*)h->W, rW, d, (Tc*)h->F[d], s))) {
+      return st;
+    }
     fs.f[d] = make_view((const Tc*)h->F[d], face_region(h, d));
     fs.has[d] = 1;
     fs.neg_inv_h[d] = h->neg_inv_h[d];
