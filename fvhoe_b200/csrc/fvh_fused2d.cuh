@@ -143,10 +143,19 @@ template <typename Tc, int TX, int TY>
 __device__ __forceinline__ void pointwise_tile(const double* __restrict__ u, const Geo& g, int x0, int y0, Tc* Pw,
                                                const Phys<Tc>& ph) {
   constexpr int PX = TX + 4, PY = TY + 4;
+  // tiles inside the grid read the state directly, the others through the ghost maps
+  const bool inside = !g.slabs && x0 >= 2 && x0 + TX + 2 <= g.nx && y0 >= 2 && y0 + TY + 2 <= g.ny;
+  const int plane = g.nx * g.ny;
   for (int i = threadIdx.x; i < PX * PY; i += blockDim.x) {
     const int r = i / PY, q = i - r * PY;
     Tc uc[5], w[5];
-    load_state2<Tc>(u, g, x0 - 2 + r, y0 - 2 + q, uc);
+    if (inside) {
+      const double* p = u + (x0 - 2 + r) * g.ny + y0 - 2 + q;
+#pragma unroll
+      for (int v = 0; v < 5; ++v) uc[v] = (Tc)p[v * plane];
+    } else {
+      load_state2<Tc>(u, g, x0 - 2 + r, y0 - 2 + q, uc);
+    }
     to_primitives(ph, 5, uc, w);
 #pragma unroll
     for (int v = 0; v < 5; ++v) Pw[(v * PX + r) * PY + q] = w[v];
@@ -223,11 +232,15 @@ __device__ __forceinline__ void stn(double* p, const double* o) {
   }
 }
 
-// Output rows per thread of the sweeps along the strided axis (sweepv's M).
-#ifndef FVH_MROW
-#define FVH_MROW 2
-#endif
-constexpr int MROW = FVH_MROW;
+// Output rows per thread of the sweeps along the strided axis (sweepv's M),
+// as measured fastest on B200 (KH 2048^2 p=5 and 4096^2 p=7, both forms, all
+// variants bit-identical): three in the FP64 primitive tiles, one in the FP32
+// ones; in the flux tile two for the 7- and 9-tap rules of p >= 6, else one.
+template <typename Tc>
+constexpr int mrow_prims() {
+  return sizeof(Tc) == 8 ? 3 : 1;
+}
+constexpr int mrow_flux(int kc) { return kc >= 7 ? 2 : 1; }
 
 // Elements per shared-memory vector: one 16-byte access (4 floats, 2 doubles).
 template <typename Tc>
@@ -351,17 +364,33 @@ __device__ __forceinline__ void primitives_tile(const Tin* __restrict__ u, const
   using D = PrimsDims<Tc, P, OX, OY>;
   constexpr int RC = D::RC, VW = VecW<Tc>::value;
   const int nt = blockDim.x;
-  // 1. state with 2*RC ghosts around the tile: A, LX x LYS
-  for (int i = threadIdx.x; i < D::LX * D::LY; i += nt) {
-    const int r = i / D::LY, q = i - r * D::LY;
-    Tc s[5];
-    load_state2<Tc>(u, g, x0 - 2 * RC + r, y0 - 2 * RC + q, s);
+  // 1. state with 2*RC ghosts around the tile: A, LX x LYS. A tile whose
+  // loaded box lies inside the grid (most tiles) reads the state directly;
+  // the others resolve every point through the ghost maps.
+  const int lx0 = x0 - 2 * RC, ly0 = y0 - 2 * RC;
+  if (!g.slabs && lx0 >= 0 && lx0 + D::LX <= g.nx && ly0 >= 0 && ly0 + D::LY <= g.ny) {
+    const int plane = g.nx * g.ny;
+    for (int i = threadIdx.x; i < D::LX * D::LY; i += nt) {
+      const int r = i / D::LY, q = i - r * D::LY;
+      const Tin* p = u + (lx0 + r) * g.ny + ly0 + q;
+      Tin s[5];
 #pragma unroll
-    for (int v = 0; v < 5; ++v) A[(v * D::LX + r) * D::LYS + q] = s[v];
+      for (int v = 0; v < 5; ++v) s[v] = p[v * plane];
+#pragma unroll
+      for (int v = 0; v < 5; ++v) A[(v * D::LX + r) * D::LYS + q] = (Tc)s[v];
+    }
+  } else {
+    for (int i = threadIdx.x; i < D::LX * D::LY; i += nt) {
+      const int r = i / D::LY, q = i - r * D::LY;
+      Tc s[5];
+      load_state2<Tc>(u, g, lx0 + r, ly0 + q, s);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) A[(v * D::LX + r) * D::LYS + q] = s[v];
+    }
   }
   __syncthreads();
   // 2. centre sweep along X: B, CX x LYS
-  sweepv<Tc, VW, KC, 1, 0, D::CX, D::LYS / VW, D::LYS, D::LX * D::LYS, D::A, MROW>(
+  sweepv<Tc, VW, KC, 1, 0, D::CX, D::LYS / VW, D::LYS, D::LX * D::LYS, D::A, mrow_prims<Tc>()>(
       A, c.w, [&](int v, int r, int q, const Tc* acc) { stn<VW>(B + (v * D::CX + r) * D::LYS + q, acc); });
   __syncthreads();
   // 3. centre sweep along Y, then primitives: A, CX x PYS
@@ -400,7 +429,7 @@ __device__ __forceinline__ void primitives_tile(const Tin* __restrict__ u, const
   }
   __syncthreads();
   // 4. transverse sweep along X: B, OX x PYS
-  sweepv<Tc, VW, KC, 1, 0, OX, D::PYS / VW, D::PYS, D::CX * D::PYS, D::A, MROW>(
+  sweepv<Tc, VW, KC, 1, 0, OX, D::PYS / VW, D::PYS, D::CX * D::PYS, D::A, mrow_prims<Tc>()>(
       A, t.w, [&](int v, int r, int q, const Tc* acc) { stn<VW>(B + (v * OX + r) * D::PYS + q, acc); });
   __syncthreads();
   // 5. transverse sweep along Y, into A as an OX x OYS tile
@@ -608,7 +637,7 @@ __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __res
       [&](int v, int r, int q, const Tc* acc) { stn<VW>(AX + (v * D::AXR + r) * D::AXS + q, acc); });
   // Y faces: AY(r, q) at (x0-RC+r, y0-1-R+q), taps along X
   sweepv<Tc, VW, KC, 1, HY - 1 - R, D::AYR, D::AYS / VW, D::WYS, D::WX * D::WYS, D::S0 - (H - 2 * RC) * D::WYS,
-         MROW>(
+         mrow_flux(KC)>(
       Ws + (H - 2 * RC) * D::WYS, c.w,
       [&](int v, int r, int q, const Tc* acc) { stn<VW>(AY + (v * D::AYR + r) * D::AYS + q, acc); });
   __syncthreads();
@@ -709,7 +738,7 @@ __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __res
   }
   __syncthreads();
   // Y face fluxes: transverse sweep along X -> GY and G (owned faces)
-  sweepv<Tc, VW, KC, 1, 0, TX, D::GYS / VW, D::BYS, D::BYR * D::BYS, D::S0, MROW>(
+  sweepv<Tc, VW, KC, 1, 0, TX, D::GYS / VW, D::BYS, D::BYR * D::BYS, D::S0, mrow_flux(KC)>(
       BY, t.w, [&](int v, int r, int f, const Tc* acc) {
         stn<VW>(GY + (v * TX + r) * D::GYS + f, acc);
         const int x = x0 + r;

@@ -19,7 +19,6 @@
 #include <string>
 
 #include "fvh_fused2d.cuh"
-#include "fvh_fused3d.cuh"
 #include "fvh_handle.h"
 #include "fvh_profile.h"
 
@@ -407,96 +406,6 @@ void launch_detect(const fvh_handle* h, const View<const Tc>& w, const View<cons
 }
 
 // ---------------------------------------------------------------------------
-// fused 3D passes (fvh_fused3d.cuh): three active axes, five variables, the
-// same degree p <= 5 on every axis, no Dirichlet sides; the generic path's six
-// sweeps of a primitive pass in one tiled launch, and its four sweeps and face
-// solve of a direction's flux pass in another, bit for bit the same results
-// ---------------------------------------------------------------------------
-inline bool fused3d_prims_eligible(const fvh_handle* h) {
-  return h->cfg.kernel_path != FVH_PATH_GENERIC && h->ndim == 3 && h->nv == 5 && !h->grid.slabs &&
-         h->p[0] == h->p[1] && h->p[1] == h->p[2] && h->p[0] <= 5;
-}
-
-template <typename Tc>
-struct Fused3Tiles;
-template <>
-struct Fused3Tiles<float> {
-  static constexpr int OX = 8, OY = 8, OZ = 16;
-};
-template <>
-struct Fused3Tiles<double> {
-  static constexpr int OX = 8, OY = 4, OZ = 16;
-};
-
-template <typename Tc, int P, bool REDUCE>
-int prims3d_p(fvh_handle* h, const double* state, int g, Tc* dst, const ReduceSpec& rs, cudaStream_t s) {
-  using T = Fused3Tiles<Tc>;
-  constexpr int KC = 2 * (P / 2) + 1;
-  using D = f3::Prims3Dims<Tc, P, T::OX, T::OY, T::OZ>;
-  const size_t smem = (size_t)D::TOTAL * sizeof(Tc);
-  auto kern = f3::k3_primitives<Tc, P, T::OX, T::OY, T::OZ, KC, REDUCE, double>;
-  cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const Region rW = padded_region(h, g);
-  const dim3 grid((rW.n[2] + T::OZ - 1) / T::OZ, (rW.n[1] + T::OY - 1) / T::OY, (rW.n[0] + T::OX - 1) / T::OX);
-  const double pts = (double)region_points(rW);
-  LaunchScope scope(KK_CENTRE, (double)h->n[0] * h->n[1] * h->n[2] * 5 * 8.0 + pts * 5 * sizeof(Tc), s);
-  kern<<<grid, 256, smem, s>>>(state, h->grid, make_view(dst, rW), g, device_rule<Tc, KC>(centre_rule(P)),
-                               device_rule<Tc, KC>(transverse_rule(P)), make_phys<Tc>(h), rs, h->sc);
-  return set_cuda_error(h, "fused 3D primitives");
-}
-
-template <typename Tc, bool REDUCE>
-int prims3d(fvh_handle* h, const double* state, int g, Tc* dst, const ReduceSpec& rs, cudaStream_t s) {
-  switch (h->p[0]) {
-    case 0: return prims3d_p<Tc, 0, REDUCE>(h, state, g, dst, rs, s);
-    case 1: return prims3d_p<Tc, 1, REDUCE>(h, state, g, dst, rs, s);
-    case 2: return prims3d_p<Tc, 2, REDUCE>(h, state, g, dst, rs, s);
-    case 3: return prims3d_p<Tc, 3, REDUCE>(h, state, g, dst, rs, s);
-    case 4: return prims3d_p<Tc, 4, REDUCE>(h, state, g, dst, rs, s);
-    default: return prims3d_p<Tc, 5, REDUCE>(h, state, g, dst, rs, s);
-  }
-}
-
-template <typename Tc, int P, int D>
-int flux3d_pd(fvh_handle* h, Tc* Fd, cudaStream_t s) {
-  using T = Fused3Tiles<Tc>;
-  constexpr int R = (P + 1) / 2, KC = 2 * (P / 2) + 1, KF = 2 * R + 1;
-  using Dm = f3::Flux3Dims<Tc, P, D, T::OX, T::OY, T::OZ>;
-  const size_t smem = (size_t)Dm::TOTAL * sizeof(Tc);
-  auto kern = f3::k3_fluxes<Tc, P, D, T::OX, T::OY, T::OZ, KC, KF>;
-  cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const Region rf = face_region(h, D);
-  const dim3 grid((rf.n[2] + T::OZ - 1) / T::OZ, (rf.n[1] + T::OY - 1) / T::OY, (rf.n[0] + T::OX - 1) / T::OX);
-  const double cells = (double)h->n[0] * h->n[1] * h->n[2];
-  LaunchScope scope(KK_FACE, cells * 5 * sizeof(Tc) + (double)region_points(rf) * 5 * sizeof(Tc), s);
-  kern<<<grid, 256, smem, s>>>(make_view((const Tc*)h->W, padded_region(h, h->gW)), h->gW, h->grid, make_view(Fd, rf),
-                               device_rule<Tc, KC>(centre_rule(P)), device_rule<Tc, KC>(transverse_rule(P)),
-                               device_rule<Tc, KF>(left_face_rule(P)), device_rule<Tc, KF>(right_face_rule(P)),
-                               make_phys<Tc>(h));
-  return set_cuda_error(h, "fused 3D fluxes");
-}
-
-template <typename Tc, int P>
-int flux3d_p(fvh_handle* h, int d, Tc* Fd, cudaStream_t s) {
-  if (d == 0) return flux3d_pd<Tc, P, 0>(h, Fd, s);
-  if (d == 1) return flux3d_pd<Tc, P, 1>(h, Fd, s);
-  return flux3d_pd<Tc, P, 2>(h, Fd, s);
-}
-
-// High-order face fluxes along d of a fused-3D-eligible handle from W.
-template <typename Tc>
-int flux3d(fvh_handle* h, int d, Tc* Fd, cudaStream_t s) {
-  switch (h->p[0]) {
-    case 0: return flux3d_p<Tc, 0>(h, d, Fd, s);
-    case 1: return flux3d_p<Tc, 1>(h, d, Fd, s);
-    case 2: return flux3d_p<Tc, 2>(h, d, Fd, s);
-    case 3: return flux3d_p<Tc, 3>(h, d, Fd, s);
-    case 4: return flux3d_p<Tc, 4>(h, d, Fd, s);
-    default: return flux3d_p<Tc, 5>(h, d, Fd, s);
-  }
-}
-
-// ---------------------------------------------------------------------------
 // one stage
 // ---------------------------------------------------------------------------
 template <typename Tc, int NV>
@@ -517,12 +426,7 @@ int run_stage_t(fvh_handle* h, const StageCall& c, cudaStream_t s) {
   rs.ext_box = padded_region(h, 3);
   rs.ndim = (double)h->ndim;
   const Region rW = padded_region(h, h->gW);
-  const bool fused3 = fused3d_prims_eligible(h);
-  if (fused3) {
-    if ((st = prims3d<Tc, true>(h, c.stage_in, h->gW, (Tc*)h->W, rs, s))) return st;
-  } else if ((st = primitive_pass<Tc, NV>(h, c.stage_in, h->gW, (Tc*)h->W, rs, true, true, s))) {
-    return st;
-  }
+  if ((st = primitive_pass<Tc, NV>(h, c.stage_in, h->gW, (Tc*)h->W, rs, true, true, s))) return st;
   // 2. dt
   {
     LaunchScope scope(KK_SMALL, 0.0, s);
@@ -533,11 +437,7 @@ int run_stage_t(fvh_handle* h, const StageCall& c, cudaStream_t s) {
   FluxSet<Tc> fs{};
   for (int d = 0; d < 3; ++d) {
     if (!h->active[d]) continue;
-    if (fused3) {
-      if ((st = flux3d<Tc>(h, d, (Tc*)h->F[d], s))) return st;
-    } else if ((st = flux_pass<Tc, NV>(h, (const Tc*)h->W, rW, d, (Tc*)h->F[d], s))) {
-      return st;
-    }
+    if ((st = flux_pass<Tc, NV>(h, (const Tc*)h->W, rW, d, (Tc*)h->F[d], s))) return st;
     fs.f[d] = make_view((const Tc*)h->F[d], face_region(h, d));
     fs.has[d] = 1;
     fs.neg_inv_h[d] = h->neg_inv_h[d];
@@ -557,11 +457,7 @@ int run_stage_t(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     }
     if ((st = set_cuda_error(h, "candidate"))) return st;
     ReduceSpec none{};
-    if (fused3) {
-      if ((st = prims3d<Tc, false>(h, h->Us, 3, (Tc*)h->Ws, none, s))) return st;
-    } else if ((st = primitive_pass<Tc, NV>(h, h->Us, 3, (Tc*)h->Ws, none, false, true, s))) {
-      return st;
-    }
+    if ((st = primitive_pass<Tc, NV>(h, h->Us, 3, (Tc*)h->Ws, none, false, true, s))) return st;
     DetectSpec ds{};
     ds.nad_global = cfg.nad_global;
     ds.nad_relative = cfg.nad_relative;

@@ -309,24 +309,3 @@ def test_host_state_steps_equal_device_steps(precision):
             assert np.array_equal(host.numpy(), dev.am.get_numpy("u"))
     assert lib.fvh_host_sync(None) == _capi.ERR_ARG
 
-
-@pytest.mark.parametrize("p", [1, 2, 3, 4, 5])
-@pytest.mark.parametrize("n", [(20, 18, 17), (33, 16, 24)])
-def test_fused3d_primitives_equal_generic_fp64(p, n):
-    """3D problems run their primitive passes as one tiled kernel when eligible
-    ("auto"); the steps equal the generic sweeps bit for bit for every degree
-    it covers, on ragged grids with mixed periodic, outflow and reflective
-    sides."""
-    from fvhoe_b200 import BoundaryCondition, EulerSolver, SedovBlast
-
-    kw = dict(w0=SedovBlast(dims="xyz"), conservative_ic=True, fv_ic=True, nx=n[0], ny=n[1], nz=n[2], px=p, py=p,
-              pz=p, gamma=1.4, riemann_solver="llf", CFL=0.5,
-              bc=BoundaryCondition(x=("reflective", "outflow"), y="periodic", z=("outflow", "reflective")),
-              a_posteriori_slope_limiting=True, NAD=1e-4, progress_bar=False)
-    fused = EulerSolver(kernel_path="auto", **kw)
-    generic = EulerSolver(kernel_path="generic", **kw)
-    fused.ssprk3(n=2)
-    generic.ssprk3(n=2)
-    assert fused.t == generic.t
-    assert np.array_equal(fused.am.get_numpy("u"), generic.am.get_numpy("u"))
-    assert np.array_equal(fused.trouble_flags(), generic.trouble_flags())
