@@ -242,6 +242,17 @@ constexpr int mrow_prims() {
 }
 constexpr int mrow_flux(int kc) { return kc >= 7 ? 2 : 1; }
 
+// One element from global to shared memory by an asynchronous copy (4 or 8
+// bytes, cached in L1), and the wait for all of this thread's copies.
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* smem_dst, const T* gmem_src) {
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte elements");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
+               "l"(gmem_src), "n"(sizeof(T))
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Elements per shared-memory vector: one 16-byte access (4 floats, 2 doubles).
 template <typename Tc>
 struct VecW {
@@ -569,13 +580,23 @@ struct FluxDims {
   // bytes after the three regions that a block with predicted flags needs: two
   // counters and the lists of the faces that take the fallback flux
   static constexpr int LIST = 16 + 2 * ((TX + 1) * TY + TX * (TY + 1));
+  // resident blocks per SM that the shared memory allows (227 KB per SM, 128
+  // bytes of alignment slack per block), at most 4 (FP32) or 3 (FP64): the
+  // launch bounds give each thread the registers of that occupancy
+  template <typename Tc>
+  static constexpr int blocks() {
+    constexpr int cap = sizeof(Tc) == 4 ? 4 : 3;
+    constexpr int fit = (227 * 1024) / (TOTAL * (int)sizeof(Tc) + 128);
+    return fit < cap ? fit : cap;
+  }
 };
 
 // CHX, CHY: consecutive faces per thread in the two Riemann phases (sliding
 // windows along X and Y); one in FP64, whose states take twice the registers,
-// and fewer along Y for the 9-tap face rules of p = 7, 8 (no register spills)
+// and fewer along Y for the 9-tap face rules when 4 blocks per SM leave 64
+// registers (no register spills)
 template <typename Tc, int P, int TX, int TY, int KC, int KF, int CHX = (sizeof(Tc) == 4 ? 3 : 1),
-          int CHY = (sizeof(Tc) == 4 ? (KF >= 9 ? 2 : 4) : 1)>
+          int CHY = (sizeof(Tc) == 4 ? (KF >= 9 && FluxDims<P, TX, TY>::template blocks<Tc>() >= 4 ? 2 : 4) : 1)>
 __device__ __forceinline__ void tile2_fluxes(V2<const Tc> W, const double* __restrict__ u, Geo g, V2<Tc> F, V2<Tc> G,
                                              Tc* __restrict__ ustar, Rule<Tc, KC> c, Rule<Tc, KC> t,
                                              Rule<Tc, KF> lrule, Rule<Tc, KF> rrule, Phys<Tc> ph, double cx,
@@ -845,7 +866,7 @@ struct DtSpec {
 };
 
 template <typename Tc, int P, int TX, int TY, int KC, int KF>
-__global__ void __launch_bounds__(256, sizeof(Tc) == 4 ? 4 : 3)
+__global__ void __launch_bounds__(256, FluxDims<P, TX, TY>::template blocks<Tc>())
     k2_fluxes(V2<const Tc> W, const double* __restrict__ u, Geo g, V2<Tc> F, V2<Tc> G, Tc* __restrict__ ustar,
               Rule<Tc, KC> c, Rule<Tc, KC> t, Rule<Tc, KF> lrule, Rule<Tc, KF> rrule, Phys<Tc> ph, double cx,
               double cy, Scalars* __restrict__ sc, DtSpec dts, const uint8_t* __restrict__ pred, int muscl,
@@ -1251,21 +1272,25 @@ __device__ __forceinline__ void tile2_final(const double* __restrict__ stage_in,
   Tc* GY = FX + D::SF;
   const int nt = blockDim.x;
   const int x0 = by * TX, y0 = bx * TY;
-  // high-order fluxes of the tile's faces
+  // high-order fluxes of the tile's faces, copied by asynchronous
+  // global-to-shared copies (cp.async): every element of both tiles is in
+  // flight at once, no register holds it, and each thread waits for its own
+  // copies before the first barrier
   for (int i = threadIdx.x; i < (TX + 1) * TY; i += nt) {
     const int f = i / TY, q = i - f * TY;
     const int x = min(x0 + f, g.nx), y = min(y0 + q, g.ny - 1);
     const Tc* p = F.p + F.at(x, y);
 #pragma unroll
-    for (int v = 0; v < 5; ++v) FX[(v * (TX + 1) + f) * TY + q] = p[v * F.vs];
+    for (int v = 0; v < 5; ++v) cp_async_elem(&FX[(v * (TX + 1) + f) * TY + q], p + v * F.vs);
   }
   for (int i = threadIdx.x; i < TX * (TY + 1); i += nt) {
     const int r = i / (TY + 1), f = i - r * (TY + 1);
     const int x = min(x0 + r, g.nx - 1), y = min(y0 + f, g.ny);
     const Tc* p = G.p + G.at(x, y);
 #pragma unroll
-    for (int v = 0; v < 5; ++v) GY[(v * TX + r) * (TY + 1) + f] = p[v * G.vs];
+    for (int v = 0; v < 5; ++v) cp_async_elem(&GY[(v * TX + r) * (TY + 1) + f], p + v * G.vs);
   }
+  cp_async_wait_all();
   // fallback at the faces of troubled cells; with predicted flags, faces next
   // to a predicted cell already hold their fallback flux (k2_fluxes) and only
   // the faces of missed cells are revised here. Revising face by face from the
