@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <string>
+#include <type_traits>
 
 #include "fvh_fused2d.cuh"
 #include "fvh_stream3d.cuh"
@@ -409,11 +410,15 @@ void launch_detect(const fvh_handle* h, const View<const Tc>& w, const View<cons
 // ---------------------------------------------------------------------------
 // streaming 3D primitive pass (fvh_stream3d.cuh): three active axes, five
 // variables, the same degree p <= 3 on every axis, no Dirichlet sides; the six
-// sweeps of a primitive pass in one launch, bit for bit the same W
+// sweeps of a primitive pass in one launch, bit for bit the same W. Taken in
+// FP32 only: on Sedov 256^3 it measured 21.7 ms per step against the generic
+// sweeps' 22.3 in FP32, but 40.9 against 38.9 in FP64, where the FP64 planes
+// leave room for two blocks per SM.
 // ---------------------------------------------------------------------------
+template <typename Tc>
 inline bool stream3d_eligible(const fvh_handle* h) {
-  return h->cfg.kernel_path != FVH_PATH_GENERIC && h->ndim == 3 && h->nv == 5 && !h->grid.slabs &&
-         h->p[0] == h->p[1] && h->p[1] == h->p[2] && h->p[0] <= 3;
+  return std::is_same<Tc, float>::value && h->cfg.kernel_path != FVH_PATH_GENERIC && h->ndim == 3 &&
+         h->nv == 5 && !h->grid.slabs && h->p[0] == h->p[1] && h->p[1] == h->p[2] && h->p[0] <= 3;
 }
 
 template <typename Tc>
@@ -482,7 +487,7 @@ int run_stage_t(fvh_handle* h, const StageCall& c, cudaStream_t s) {
   rs.ext_box = padded_region(h, 3);
   rs.ndim = (double)h->ndim;
   const Region rW = padded_region(h, h->gW);
-  const bool stream3 = stream3d_eligible(h);
+  const bool stream3 = stream3d_eligible<Tc>(h);
   if (stream3) {
     if ((st = stream3d<Tc, true>(h, c.stage_in, h->gW, (Tc*)h->W, rs, s))) return st;
   } else if ((st = primitive_pass<Tc, NV>(h, c.stage_in, h->gW, (Tc*)h->W, rs, true, true, s))) {

@@ -8,8 +8,9 @@
 // chunk of output planes, so every state plane is read from memory once per
 // tile instead of once per x tile, and the x-direction sweeps run on rings of
 // planes kept in shared memory:
-//   plane i of the state arrives by asynchronous copies (cp.async, raw FP64)
-//   into a ring of 2RC+2 planes (one plane ahead of its use);
+//   plane i of the state is loaded through registers (its loads in flight
+//   while the plane before it is computed), sign-corrected and converted,
+//   into a ring of 2RC+2 planes;
 //   C(i) = C_z C_y C_x u at plane i (RC = p / 2, the centre rule's radius),
 //   converted to primitives, into a ring of 2RC+1 planes;
 //   W(i-RC) = T_z T_y T_x of the primitive ring, written to global memory.
@@ -33,20 +34,17 @@ struct Stream3Dims {
   static constexpr int NU = 2 * RC + 2;                     // state ring (one plane ahead)
   static constexpr int NP = 2 * RC + 1;                     // primitive ring
   static constexpr int PL = LY * LZ, PC = CY * CZ;
-  // bytes: state ring (FP64), x-swept plane A (5 LY LZ), y-swept plane B
+  // bytes: state ring (compute type), x-swept plane A (5 LY LZ), y-swept plane B
   // (5 CY LZ), primitive ring (NP x 5 CY CZ), offsets and flip bits of the
   // plane tile's y-z points
-  static constexpr int U_BYTES = NU * 5 * PL * 8;
+  static constexpr int U_BYTES = NU * 5 * PL * (int)sizeof(Tc);
+  static constexpr int LOADS = (5 * PL + 255) / 256;  // state values a thread stages per plane
   static constexpr int A_ELEMS = 5 * PL, B_ELEMS = 5 * CY * LZ, R_ELEMS = NP * 5 * PC;
   static constexpr int BYTES = U_BYTES + (A_ELEMS + B_ELEMS + R_ELEMS) * (int)sizeof(Tc) + PL * 4 + PL + 16;
+  // resident blocks the shared memory allows (at most three), for the launch bounds
+  static constexpr int FIT = (228 * 1024) / (BYTES + 1024);
+  static constexpr int BLOCKS = FIT < 1 ? 1 : (FIT > 3 ? 3 : FIT);
 };
-
-__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
-               "l"(gmem_src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 __device__ __forceinline__ int ring(int i, int n) {
   const int r = i % n;
@@ -58,20 +56,19 @@ __device__ __forceinline__ int ring(int i, int n) {
 // along y) and its chunk of output planes along x (blockIdx.z). REDUCE: the
 // CFL maximum over rs.cfl_box and the per-variable extrema over rs.ext_box.
 template <typename Tc, int P, int OY, int OZ, int KC, bool REDUCE>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, (Stream3Dims<Tc, P, OY, OZ>::BLOCKS))
     k3s_primitives(const double* __restrict__ u, Grid grid, View<Tc> W, int g, int chunk, Rule<Tc, KC> c,
                    Rule<Tc, KC> t, Phys<Tc> ph, ReduceSpec rs, Scalars* __restrict__ sc) {
   using D = Stream3Dims<Tc, P, OY, OZ>;
   constexpr int RC = D::RC, LZ = D::LZ, CY = D::CY, CZ = D::CZ, PL = D::PL, PC = D::PC, NU = D::NU,
                 NP = D::NP;
   extern __shared__ __align__(16) unsigned char smem[];
-  double* const U = reinterpret_cast<double*>(smem);  // NU x 5 x PL
+  Tc* const U = reinterpret_cast<Tc*>(smem);  // NU x 5 x PL: state planes, sign-corrected, converted
   Tc* const A = reinterpret_cast<Tc*>(smem + D::U_BYTES);
   Tc* const B = A + D::A_ELEMS;
   Tc* const R = B + D::B_ELEMS;
   int* const off = reinterpret_cast<int*>(R + D::R_ELEMS);              // y-z source offset of each plane point
   unsigned char* const fl = reinterpret_cast<unsigned char*>(off + PL);  // bit 0: y mirror flips, bit 1: z
-  __shared__ int xflip[NU];
   const int n0 = grid.n[0], n1 = grid.n[1], n2 = grid.n[2];
   const int gmax = g + 2 * RC;
   const int plane = n0 * n1 * n2;
@@ -91,21 +88,42 @@ __global__ void __launch_bounds__(256)
     fl[e] = (unsigned char)((fy ? 1 : 0) | (fz ? 2 : 0));
   }
   __syncthreads();
-  // asynchronous copies of state plane xi into its ring slot
-  auto issue = [&](int xi) {
+  // a state plane is staged through registers: the loads of plane xi are
+  // issued early (fetch), and the values stored into the ring later (store),
+  // each sign-corrected in FP64 (the reflective mirror flips) and converted
+  double stage[D::LOADS];
+  bool stage_fx = false;
+  auto fetch = [&](int xi) {
     const int xc = min(max(xi, -gmax), n0 + gmax - 1);
-    bool fx = false;
-    const int jx = ghost_source(xc, n0, grid.bc[0][0], grid.bc[0][1], fx);
-    const int slot = ring(xi, NU);
-    if (threadIdx.x == 0) xflip[slot] = fx ? 1 : 0;
-    double* dst = U + slot * 5 * PL;
+    stage_fx = false;  // ghost_source only sets the flag
+    const int jx = ghost_source(xc, n0, grid.bc[0][0], grid.bc[0][1], stage_fx);
     const double* src = u + (size_t)jx * n1 * n2;
-    for (int idx = threadIdx.x; idx < 5 * PL; idx += blockDim.x) {
-      const int v = idx / PL, e = idx - v * PL;
-      cp_async8(dst + idx, src + (size_t)v * plane + off[e]);
+#pragma unroll
+    for (int m = 0; m < D::LOADS; ++m) {
+      const int idx = threadIdx.x + 256 * m;
+      if (idx < 5 * PL) {
+        const int v = idx / PL, e = idx - v * PL;
+        stage[m] = src[(size_t)v * plane + off[e]];
+      }
     }
   };
-  for (int xi = xb - 2 * RC; xi <= xb; ++xi) issue(xi);
+  auto store = [&](int xi) {
+    Tc* dst = U + ring(xi, NU) * 5 * PL;
+#pragma unroll
+    for (int m = 0; m < D::LOADS; ++m) {
+      const int idx = threadIdx.x + 256 * m;
+      if (idx < 5 * PL) {
+        const int v = idx / PL, e = idx - v * PL;
+        double d = stage[m];
+        if ((v == 1 && stage_fx) || (v == 2 && (fl[e] & 1)) || (v == 3 && (fl[e] & 2))) d = -d;
+        dst[idx] = (Tc)d;
+      }
+    }
+  };
+  for (int xi = xb - 2 * RC; xi <= xb; ++xi) {
+    fetch(xi);
+    store(xi);
+  }
   unsigned long long cfl_key = 0ull, kmax[5], kmin[5];
 #pragma unroll
   for (int v = 0; v < 5; ++v) {
@@ -113,23 +131,19 @@ __global__ void __launch_bounds__(256)
     kmin[v] = ~0ull;
   }
   for (int i = xb - RC; i < xe + RC; ++i) {
-    cp_async_wait();
-    __syncthreads();  // state planes i-RC .. i+RC and their flip flags are in place
-    if (i + RC + 1 <= xe - 1 + 2 * RC) issue(i + RC + 1);  // its slot held plane i-RC-1, no longer read
-    // centre sweep along x (the state, sign-corrected in FP64, then converted)
+    __syncthreads();  // state planes i-RC .. i+RC are in the ring
+    const bool ahead = i + RC + 1 <= xe - 1 + 2 * RC;
+    if (ahead) fetch(i + RC + 1);  // in flight while this plane is computed
+    // centre sweep along x
     for (int idx = threadIdx.x; idx < 5 * PL; idx += blockDim.x) {
-      const int v = idx / PL, e = idx - v * PL;
-      const bool fyz = (v == 2 && (fl[e] & 1)) || (v == 3 && (fl[e] & 2));
       Tc acc = Tc(0);
 #pragma unroll
-      for (int k = 0; k < KC; ++k) {
-        const int slot = ring(i - RC + k, NU);
-        double d = U[slot * 5 * PL + idx];
-        if (fyz || (v == 1 && xflip[slot])) d = -d;
-        acc = acc + c.w[k] * (Tc)d;
-      }
+      for (int k = 0; k < KC; ++k) acc = acc + c.w[k] * U[ring(i - RC + k, NU) * 5 * PL + idx];
       A[idx] = acc;
     }
+    // plane i+RC+1 into the slot of plane i-RC-1, read by no phase after this
+    // iteration's first barrier
+    if (ahead) store(i + RC + 1);
     __syncthreads();
     // centre sweep along y: B (5 x CY x LZ)
     for (int idx = threadIdx.x; idx < 5 * CY * LZ; idx += blockDim.x) {
@@ -214,7 +228,6 @@ __global__ void __launch_bounds__(256)
       }
     }
   }
-  cp_async_wait();
   if constexpr (REDUCE) f2::reduce_keys_and_publish(cfl_key, kmax, kmin, rs, sc);
 }
 
