@@ -761,6 +761,134 @@ __global__ void __launch_bounds__(256)
   block_count_add(count, &sc->troubled);
 }
 
+// The same detection for three active axes, with the 3^3 box extrema from a
+// sliding window: a thread owns one (i1, i2) column of the box and CH
+// consecutive cells along axis 0, and per variable takes the 3x3 extrema of
+// each plane once (9 loads), the box extrema of a cell being those of its
+// three planes (about 11 loads per cell and variable instead of 27). Minima
+// and maxima do not depend on the order they are taken in, and every other
+// quantity is formed as k_detect forms it, variable after variable, so the
+// flags and logs are the same. Grid: x over the columns, y over the chunks.
+template <typename Tc, int CH>
+__global__ void __launch_bounds__(256, 2)
+    k_detect3(View<const Tc> w, View<const Tc> ws, Box box, DetectSpec ds, Scalars* __restrict__ sc,
+              View<uint8_t> trouble, double* __restrict__ log_trouble, double* __restrict__ log_nad,
+              double* __restrict__ log_pad) {
+  const int sw0 = w.stride(0), sw1 = w.stride(1), sw2 = w.stride(2);
+  const int sws[3] = {ws.stride(0), ws.stride(1), ws.stride(2)};
+  const Tc neg_eps = (Tc)(-ds.nad_eps);
+  const Tc lo_fac = (Tc)(1.0 - ds.nad_eps), hi_fac = (Tc)(1.0 + ds.nad_eps);
+  const Tc sed_eps = (Tc)ds.sed_eps;
+  unsigned int count = 0;
+  const uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
+  const int x0 = box.lo[0] + (int)blockIdx.y * CH;
+  const int ncell = min(CH, box.lo[0] + box.n[0] - x0);
+  if (col < (uint32_t)box.n[1] * box.n[2] && ncell > 0) {
+    const int i1 = box.lo[1] + (int)(col / (uint32_t)box.n[2]);
+    const int i2 = box.lo[2] + (int)(col % (uint32_t)box.n[2]);
+    Tc ind_min[CH], pad_ind[CH];
+    unsigned int nad_bits = 0u;
+#pragma unroll
+    for (int c = 0; c < CH; ++c) {
+      ind_min[c] = Tc(0);
+      pad_ind[c] = Tc(0);
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      // the variable's global NAD bounds (formed as k_detect forms them)
+      const double vmax = key_value(sc->vmax_key[v]);
+      const double vmin = key_value(sc->vmin_key[v]);
+      const Tc grange = (Tc)(vmax - vmin);
+      const Tc glower = (Tc)((1.0 - ds.nad_eps) * vmin);
+      const Tc gupper = (Tc)((1.0 + ds.nad_eps) * vmax);
+      const Tc* pw = w.p + v * w.vs + w.at(x0, i1, i2);
+      const Tc* pws0 = ws.p + v * ws.vs + ws.at(x0, i1, i2);
+      // 3x3 extrema of the plane at offset a along axis 0 (centre first, as
+      // the box loop of k_detect starts)
+      auto plane = [&](int a, Tc& big, Tc& small) {
+        const Tc* q = pw + a * sw0;
+        big = q[0];
+        small = big;
+#pragma unroll
+        for (int b = -1; b <= 1; ++b)
+#pragma unroll
+          for (int cc = -1; cc <= 1; ++cc) {
+            const Tc x = q[b * sw1 + cc * sw2];
+            big = fmax(big, x);
+            small = fmin(small, x);
+          }
+      };
+      Tc bm, sm, b0, s0, bp, sp;
+      plane(-1, bm, sm);
+      plane(0, b0, s0);
+#pragma unroll
+      for (int c = 0; c < CH; ++c) {
+        if (c < ncell) {
+          plane(c + 1, bp, sp);
+          const Tc big = fmax(fmax(bm, b0), bp), small = fmin(fmin(sm, s0), sp);
+          const Tc* pws = pws0 + c * sws[0];
+          const Tc xs = pws[0];
+          Tc ind;
+          bool tv;
+          if (ds.nad_relative) {
+            const Tc range = ds.nad_global ? grange : big - small;
+            ind = xs - small;
+            ind = fmin(ind, big - xs);
+            tv = ind < neg_eps * range;
+          } else {
+            const Tc lower = ds.nad_global ? glower : lo_fac * small;
+            const Tc upper = ds.nad_global ? gupper : hi_fac * big;
+            ind = fmin(xs - lower, upper - xs);
+            tv = ind < Tc(0);
+          }
+          if (tv && ds.sed) {
+            bool below = false;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+              if (below) break;
+              Tc line[7];
+#pragma unroll
+              for (int m = 0; m < 7; ++m) line[m] = pws[(m - 3) * sws[k]];
+              below = sed_line_below_one(line, sed_eps);
+            }
+            tv = below;
+          }
+          if (!((ds.nad_var_mask >> v) & 1)) tv = false;
+          if (tv) nad_bits |= 1u << c;
+          ind_min[c] = (v == 0) ? ind : fmin(ind_min[c], ind);
+          if (v == ds.pad_var) {
+            Tc pi = xs - (Tc)ds.pad_lo;
+            pad_ind[c] = fmin(pi, (Tc)ds.pad_hi - xs);
+          }
+          bm = b0;
+          sm = s0;
+          b0 = bp;
+          s0 = sp;
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < CH; ++c) {
+      if (c < ncell) {
+        const bool nad_any = (nad_bits >> c) & 1u;
+        const bool pad_trouble = pad_ind[c] < Tc(0);
+        bool t = pad_trouble || nad_any;
+        if (ds.force_trouble) t = true;
+        const int o = trouble.at(x0 + c, i1, i2);
+        trouble.p[o] = t ? 1 : 0;
+        count += t ? 1u : 0u;
+        if (ds.log_mode) {
+          const double lt = t ? 1.0 : 0.0;
+          const double ln = nad_any ? -(double)ind_min[c] : 0.0;
+          const double lp = pad_trouble ? -(double)pad_ind[c] : 0.0;
+          log_write(ds, o, lt, ln, lp, log_trouble, log_nad, log_pad);
+        }
+      }
+    }
+  }
+  block_count_add(count, &sc->troubled);
+}
+
 // ---------------------------------------------------------------------------
 // Pointwise primitives of the stage input over the interior and 2 ghost
 // cells: the fallback scheme's FV primitives, because its p = 1 centre and

@@ -400,9 +400,17 @@ int flux_pass(fvh_handle* h, const Tc* W, Region rW, int d, Tc* Fd, cudaStream_t
 // ---------------------------------------------------------------------------
 int convex_weights(fvh_handle* h, cudaStream_t s);
 
+// Three active axes take the sliding-window kernel (k_detect3, the same flags
+// and logs) unless the generic kernels are asked for.
 template <int NDIM, typename Tc>
 void launch_detect(const fvh_handle* h, const View<const Tc>& w, const View<const Tc>& ws, const Box& box,
                    const DetectSpec& ds, const View<uint8_t>& tr, cudaStream_t s) {
+  if (NDIM == 3 && h->cfg.kernel_path != FVH_PATH_GENERIC) {
+    constexpr int CH = 8;
+    const dim3 grid((unsigned)(((size_t)box.n[1] * box.n[2] + 255) / 256), (unsigned)((box.n[0] + CH - 1) / CH));
+    k_detect3<Tc, CH><<<grid, 256, 0, s>>>(w, ws, box, ds, h->sc, tr, h->logs[0], h->logs[1], h->logs[2]);
+    return;
+  }
   k_detect<Tc, NDIM><<<blocks_for(box.count), 256, 0, s>>>(w, ws, box, ds, h->sc, tr, h->logs[0], h->logs[1],
                                                            h->logs[2]);
 }
