@@ -765,12 +765,13 @@ __global__ void __launch_bounds__(256)
 // sliding window: a thread owns one (i1, i2) column of the box and CH
 // consecutive cells along axis 0, and per variable takes the 3x3 extrema of
 // each plane once (9 loads), the box extrema of a cell being those of its
-// three planes (about 11 loads per cell and variable instead of 27). Minima
+// three planes (9 (CH + 2) / CH loads per cell and variable instead of 27,
+// at 80 registers for three blocks per SM). Minima
 // and maxima do not depend on the order they are taken in, and every other
 // quantity is formed as k_detect forms it, variable after variable, so the
 // flags and logs are the same. Grid: x over the columns, y over the chunks.
 template <typename Tc, int CH>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, 3)
     k_detect3(View<const Tc> w, View<const Tc> ws, Box box, DetectSpec ds, Scalars* __restrict__ sc,
               View<uint8_t> trouble, double* __restrict__ log_trouble, double* __restrict__ log_nad,
               double* __restrict__ log_pad) {
@@ -970,6 +971,83 @@ __global__ void __launch_bounds__(256)
     riemann_flux<NVA>(ph, nv, wl, wr, d, flo);
     Tc* o = F.p + F.at(i[0], i[1], i[2]);
     for (int v = 0; v < nv; ++v) o[v * F.vs] = (Tc(1) - theta) * o[v * F.vs] + theta * flo[v];
+  }
+}
+
+// The same fallback without the pointwise pass and without idle lanes (the
+// faces' own flags, no convex weights): a block takes 1024 faces at a time,
+// gathers the faces next to a troubled cell into a shared list (one atomic
+// per warp) and solves the list with whole warps, converting the four cells
+// a face reads from the stage input as k_pointwise_primitives converts them.
+// Every face value equals k_fallback's.
+template <typename Tc, int NV>
+__global__ void __launch_bounds__(256)
+    k_fallback_direct(const double* __restrict__ u, Grid grid, View<Tc> F, Box box, View<const uint8_t> trouble,
+                      FallbackSpec fb, Phys<Tc> ph) {
+  constexpr int NVA = VarCount<NV>::kArray;
+  constexpr int CHUNK = 1024;
+  __shared__ uint32_t list[CHUNK];
+  __shared__ int count;
+  const int nv = VarCount<NV>::get(ph);
+  const int d = fb.d;
+  const int st = trouble.stride(d);
+  const int lane = threadIdx.x & 31;
+  for (uint32_t base = blockIdx.x * CHUNK; base < box.count; base += gridDim.x * CHUNK) {
+    if (threadIdx.x == 0) count = 0;
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < CHUNK; k += blockDim.x) {
+      const uint32_t idx = base + k;
+      bool on = false;
+      if (idx < box.count) {
+        int i0, i1, i2;
+        box_point(box, idx, i0, i1, i2);
+        const int j = d == 0 ? i0 : (d == 1 ? i1 : i2);
+        const int ot = trouble.at(i0, i1, i2);
+        on = (j >= 1 && trouble.p[ot - st]) || (j < fb.nd && trouble.p[ot]);
+      }
+      const unsigned int ballot = __ballot_sync(0xffffffffu, on);
+      int wbase = 0;
+      if (lane == 0 && ballot) wbase = atomicAdd(&count, __popc(ballot));
+      wbase = __shfl_sync(0xffffffffu, wbase, 0);
+      if (on) list[wbase + __popc(ballot & ((1u << lane) - 1u))] = idx;
+    }
+    __syncthreads();
+    const int n = count;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      int i[3];
+      box_point(box, list[k], i[0], i[1], i[2]);
+      // primitives at cells j-2 .. j+1 along d
+      Tc a[4][NVA];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        int c[3] = {i[0], i[1], i[2]};
+        c[d] += m - 2;
+        Tc uc[NVA];
+        load_state<Tc>(u, grid, nv, c[0], c[1], c[2], uc);
+        to_primitives(ph, nv, uc, a[m]);
+      }
+      Tc wl[NVA], wr[NVA];
+      for (int v = 0; v < nv; ++v) {
+        const Tc a0 = a[0][v], a1 = a[1][v], a2 = a[2][v], a3 = a[3][v];
+        if (fb.muscl && fb.limiter == LIMITER_NONE) {
+          wl[v] = ((Tc(0) + Tc(-0.25) * a0) + Tc(1) * a1) + Tc(0.25) * a2;
+          wr[v] = ((Tc(0) + Tc(0.25) * a1) + Tc(1) * a2) + Tc(-0.25) * a3;
+        } else if (fb.muscl) {
+          const Tc sl = limited_slope(a1 - a0, a2 - a1, fb.limiter);
+          const Tc sr = limited_slope(a2 - a1, a3 - a2, fb.limiter);
+          wl[v] = a1 + Tc(0.5) * sl;
+          wr[v] = a2 - Tc(0.5) * sr;
+        } else {
+          wl[v] = a1;
+          wr[v] = a2;
+        }
+      }
+      Tc flo[NVA];
+      riemann_flux<NVA>(ph, nv, wl, wr, d, flo);
+      Tc* o = F.p + F.at(i[0], i[1], i[2]);
+      for (int v = 0; v < nv; ++v) o[v * F.vs] = (Tc(1) - Tc(1)) * o[v * F.vs] + Tc(1) * flo[v];
+    }
+    __syncthreads();  // the list is read before the next chunk resets it
   }
 }
 
