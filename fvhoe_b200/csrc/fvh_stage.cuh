@@ -420,9 +420,9 @@ void launch_detect(const fvh_handle* h, const View<const Tc>& w, const View<cons
 // streaming 3D primitive pass (fvh_stream3d.cuh): three active axes, five
 // variables, the same degree p <= 3 on every axis, no Dirichlet sides; the six
 // sweeps of a primitive pass in one launch, bit for bit the same W. Taken in
-// FP32 only: on Sedov 256^3 it measured 21.7 ms per step against the generic
-// sweeps' 22.3 in FP32, but 40.9 against 38.9 in FP64, where the FP64 planes
-// leave room for two blocks per SM.
+// FP32 only: on Sedov 256^3 its two launches per stage took 8.4 ms per step
+// against 9.2 ms of generic sweeps in FP32, but 15.6 against 14.5 in FP64
+// (three blocks per SM either way).
 // ---------------------------------------------------------------------------
 template <typename Tc>
 inline bool stream3d_eligible(const fvh_handle* h) {

@@ -10,7 +10,7 @@
 // planes kept in shared memory:
 //   plane i of the state is loaded through registers (its loads in flight
 //   while the plane before it is computed), sign-corrected and converted,
-//   into a ring of 2RC+2 planes;
+//   into a ring of 2RC+1 planes;
 //   C(i) = C_z C_y C_x u at plane i (RC = p / 2, the centre rule's radius),
 //   converted to primitives, into a ring of 2RC+1 planes;
 //   W(i-RC) = T_z T_y T_x of the primitive ring, written to global memory.
@@ -31,7 +31,7 @@ struct Stream3Dims {
   static constexpr int RC = P / 2;
   static constexpr int LY = OY + 4 * RC, LZ = OZ + 4 * RC;  // state plane tile
   static constexpr int CY = OY + 2 * RC, CZ = OZ + 2 * RC;  // after the centre sweeps
-  static constexpr int NU = 2 * RC + 2;                     // state ring (one plane ahead)
+  static constexpr int NU = 2 * RC + 1;                     // state ring (the centre rule's planes)
   static constexpr int NP = 2 * RC + 1;                     // primitive ring
   static constexpr int PL = LY * LZ, PC = CY * CZ;
   // bytes: state ring (compute type), x-swept plane A (5 LY LZ), y-swept plane B
@@ -141,10 +141,10 @@ __global__ void __launch_bounds__(256, (Stream3Dims<Tc, P, OY, OZ>::BLOCKS))
       for (int k = 0; k < KC; ++k) acc = acc + c.w[k] * U[ring(i - RC + k, NU) * 5 * PL + idx];
       A[idx] = acc;
     }
-    // plane i+RC+1 into the slot of plane i-RC-1, read by no phase after this
-    // iteration's first barrier
-    if (ahead) store(i + RC + 1);
     __syncthreads();
+    // plane i+RC+1 into the slot of plane i-RC, which the centre sweep above
+    // was the last to read (the next iteration's first barrier orders it)
+    if (ahead) store(i + RC + 1);
     // centre sweep along y: B (5 x CY x LZ)
     for (int idx = threadIdx.x; idx < 5 * CY * LZ; idx += blockDim.x) {
       const int v = idx / (CY * LZ), rem = idx - v * (CY * LZ), y = rem / LZ, z = rem - y * LZ;
