@@ -359,10 +359,62 @@ struct PrimsDims {
   static constexpr int PY = OY + 2 * RC;                    // after the Y centre sweep: CX x PY
   static constexpr int LYS = (LY + VW - 1) / VW * VW, PYS = (PY + VW - 1) / VW * VW, OYS = (OY + VW - 1) / VW * VW;
   static constexpr int PAD = 16;
-  // after the X transverse sweep: OX x PY; after the Y transverse sweep: OX x OY (in A)
-  static constexpr int A = Max<Max<LX * LYS, CX * PYS>::value, OX * OYS>::value * 5 + PAD;
+  // A: after the Y centre sweep CX x PY, after the Y transverse sweep OX x OY;
+  // B: after the X centre sweep CX x LY, after the X transverse sweep OX x PY
+  // (the loaded state is never stored: its columns are swept as they arrive)
+  static constexpr int A = Max<CX * PYS, OX * OYS>::value * 5 + PAD;
   static constexpr int B = Max<CX * LYS, OX * PYS>::value * 5 + PAD;
+  // row segments per column in the X centre sweep: enough column segments
+  // (five variables per column) for one per thread of a 256-thread block
+  static constexpr int NS = (256 + 5 * LY - 1) / (5 * LY);
 };
+
+// X centre sweep of a tile straight from the state: a thread takes one
+// variable of one column and SEG consecutive output rows, loads their
+// SEG + KC - 1 state rows once, in order, into a register window, and stores
+// each sum (accumulated from tap 0 upwards, as every sweep accumulates) into
+// out, CX x LYS per variable. load(r, q, v): variable v of tile row r, column q.
+template <typename Tc, int KC, int CX, int LY, int LYS, int NS, typename Load>
+__device__ __forceinline__ void centre_x_columns(Tc* __restrict__ out, const Tc* __restrict__ w, Load load) {
+  constexpr int SEG = (CX + NS - 1) / NS;
+  for (int i = threadIdx.x; i < NS * 5 * LY; i += blockDim.x) {
+    const int q = i % LY, rest = i / LY, v = rest % 5, r0 = (rest / 5) * SEG;
+    Tc win[KC];
+#pragma unroll
+    for (int k = 0; k < KC - 1; ++k) win[k] = load(r0 + k, q, v);
+#pragma unroll
+    for (int m = 0; m < SEG; ++m) {
+      if (r0 + m < CX) {
+        win[KC - 1] = load(r0 + m + KC - 1, q, v);
+        Tc acc = Tc(0);
+#pragma unroll
+        for (int k = 0; k < KC; ++k) acc = acc + w[k] * win[k];
+        out[(v * CX + r0 + m) * LYS + q] = acc;
+#pragma unroll
+        for (int k = 0; k < KC - 1; ++k) win[k] = win[k + 1];
+      }
+    }
+  }
+}
+
+// Variable v of the conserved state at a (possibly ghost) cell, as
+// load_state2 gives it.
+template <typename Tc, typename Tin>
+__device__ __forceinline__ Tc load_var2(const Tin* __restrict__ u, const Geo& g, int x, int y, int v) {
+  if (g.slabs) {
+    Tc s[5];
+    load_state2<Tc>(u, g, x, y, s);
+    return s[v];
+  }
+  x = min(max(x, -g.gmax), g.nx + g.gmax - 1);
+  y = min(max(y, -g.gmax), g.ny + g.gmax - 1);
+  bool fx = false, fy = false;
+  const int jx = ghost_source(x, g.nx, g.bcx[0], g.bcx[1], fx);
+  const int jy = ghost_source(y, g.ny, g.bcy[0], g.bcy[1], fy);
+  double val = (double)u[v * (g.nx * g.ny) + jx * g.ny + jy];
+  if ((v == 1 + g.dx && fx) || (v == 1 + g.dy && fy)) val = -val;
+  return (Tc)val;
+}
 
 // W on [x0, x0+OX) x [y0, y0+OY), computed in two shared buffers; the result
 // is left in A as an OX x OY tile with row stride OYS. Rules: centre c and
@@ -375,36 +427,22 @@ __device__ __forceinline__ void primitives_tile(const Tin* __restrict__ u, const
   using D = PrimsDims<Tc, P, OX, OY>;
   constexpr int RC = D::RC, VW = VecW<Tc>::value;
   const int nt = blockDim.x;
-  // 1. state with 2*RC ghosts around the tile: A, LX x LYS. A tile whose
-  // loaded box lies inside the grid (most tiles) reads the state directly;
-  // the others resolve every point through the ghost maps.
+  // 1. the state with 2*RC ghosts around the tile, swept along X as its
+  // columns arrive: B, CX x LYS. A tile whose loaded box lies inside the grid
+  // (most tiles) reads the state directly; the others resolve every point
+  // through the ghost maps.
   const int lx0 = x0 - 2 * RC, ly0 = y0 - 2 * RC;
   if (!g.slabs && lx0 >= 0 && lx0 + D::LX <= g.nx && ly0 >= 0 && ly0 + D::LY <= g.ny) {
     const int plane = g.nx * g.ny;
-    for (int i = threadIdx.x; i < D::LX * D::LY; i += nt) {
-      const int r = i / D::LY, q = i - r * D::LY;
-      const Tin* p = u + (lx0 + r) * g.ny + ly0 + q;
-      Tin s[5];
-#pragma unroll
-      for (int v = 0; v < 5; ++v) s[v] = p[v * plane];
-#pragma unroll
-      for (int v = 0; v < 5; ++v) A[(v * D::LX + r) * D::LYS + q] = (Tc)s[v];
-    }
+    const Tin* base = u + lx0 * g.ny + ly0;
+    centre_x_columns<Tc, KC, D::CX, D::LY, D::LYS, D::NS>(
+        B, c.w, [&](int r, int q, int v) { return (Tc)base[v * plane + r * g.ny + q]; });
   } else {
-    for (int i = threadIdx.x; i < D::LX * D::LY; i += nt) {
-      const int r = i / D::LY, q = i - r * D::LY;
-      Tc s[5];
-      load_state2<Tc>(u, g, lx0 + r, ly0 + q, s);
-#pragma unroll
-      for (int v = 0; v < 5; ++v) A[(v * D::LX + r) * D::LYS + q] = s[v];
-    }
+    centre_x_columns<Tc, KC, D::CX, D::LY, D::LYS, D::NS>(
+        B, c.w, [&](int r, int q, int v) { return load_var2<Tc>(u, g, lx0 + r, ly0 + q, v); });
   }
   __syncthreads();
-  // 2. centre sweep along X: B, CX x LYS
-  sweepv<Tc, VW, KC, 1, 0, D::CX, D::LYS / VW, D::LYS, D::LX * D::LYS, D::A, mrow_prims<Tc>()>(
-      A, c.w, [&](int v, int r, int q, const Tc* acc) { stn<VW>(B + (v * D::CX + r) * D::LYS + q, acc); });
-  __syncthreads();
-  // 3. centre sweep along Y, then primitives: A, CX x PYS
+  // 2. centre sweep along Y, then primitives: A, CX x PYS
   {
     constexpr int NG = D::PYS / VW, NW = (KC + 2 * VW - 2) / VW;
     static_assert(4 * D::CX * D::LYS + (D::CX - 1) * D::LYS + VW * (NG - 1 + NW) <= D::B,
@@ -439,11 +477,11 @@ __device__ __forceinline__ void primitives_tile(const Tin* __restrict__ u, const
     }
   }
   __syncthreads();
-  // 4. transverse sweep along X: B, OX x PYS
+  // 3. transverse sweep along X: B, OX x PYS
   sweepv<Tc, VW, KC, 1, 0, OX, D::PYS / VW, D::PYS, D::CX * D::PYS, D::A, mrow_prims<Tc>()>(
       A, t.w, [&](int v, int r, int q, const Tc* acc) { stn<VW>(B + (v * OX + r) * D::PYS + q, acc); });
   __syncthreads();
-  // 5. transverse sweep along Y, into A as an OX x OYS tile
+  // 4. transverse sweep along Y, into A as an OX x OYS tile
   sweepv<Tc, VW, KC, 0, 0, OX, D::OYS / VW, D::PYS, OX * D::PYS, D::B>(
       B, t.w, [&](int v, int r, int q, const Tc* acc) { stn<VW>(A + (v * OX + r) * D::OYS + q, acc); });
   __syncthreads();
