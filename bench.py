@@ -492,7 +492,9 @@ ENSEMBLE_KW = dict(gamma=1.4, riemann_solver="hllc", CFL=0.8, a_posteriori_slope
 
 
 def sedov_leg(args, stream, sp):
-    """The 3D Sedov configuration on the generic N-D kernels: sedov_n^3 cells of
+    """The 3D Sedov configuration on the N-D kernels (the streaming primitive
+    pass in FP32, the sliding-window detection, the compacting fallback, the
+    generic sweeps for the rest): sedov_n^3 cells of
     [0,1]^3, p = 3, LLF, SSP-RK3, CFL 0.5, reflective at the x = 0, y = 0, z = 0
     faces and outflow elsewhere, a-posteriori MUSCL with NAD and PAD, the blast
     energy in the corner cell. Timed steps (CUDA events, state on the device) of
@@ -516,7 +518,7 @@ def sedov_leg(args, stream, sp):
                            ic_on_device=True)
 
     out = {"config": f"3D Sedov {n}^3, p=3, LLF, SSP-RK3, CFL 0.5, reflective origin faces, outflow elsewhere, "
-                     "a-posteriori MUSCL with NAD + PAD; generic N-D kernels", "cells": cells}
+                     "a-posteriori MUSCL with NAD + PAD; N-D kernels", "cells": cells}
     rho = {}
     for precision in ("fp64", "fp32"):
         s = make(precision)

@@ -17,7 +17,6 @@
 #include <algorithm>
 #include <cstdio>
 #include <string>
-#include <type_traits>
 
 #include "fvh_fused2d.cuh"
 #include "fvh_stream3d.cuh"
@@ -419,40 +418,38 @@ void launch_detect(const fvh_handle* h, const View<const Tc>& w, const View<cons
 // ---------------------------------------------------------------------------
 // streaming 3D primitive pass (fvh_stream3d.cuh): three active axes, five
 // variables, the same degree p <= 3 on every axis, no Dirichlet sides; the six
-// sweeps of a primitive pass in one launch, bit for bit the same W. Taken in
-// FP32 only: on Sedov 256^3 its two launches per stage took 8.4 ms per step
-// against 9.2 ms of generic sweeps in FP32, but 15.6 against 14.5 in FP64
-// (three blocks per SM either way).
+// sweeps of a primitive pass in one launch, bit for bit the same W. On Sedov
+// 256^3 its two launches per stage take 7.4 ms per step against 9.2 ms of
+// generic sweeps in FP32, and 13.0 against 14.4 in FP64.
 // ---------------------------------------------------------------------------
-template <typename Tc>
 inline bool stream3d_eligible(const fvh_handle* h) {
-  return std::is_same<Tc, float>::value && h->cfg.kernel_path != FVH_PATH_GENERIC && h->ndim == 3 &&
-         h->nv == 5 && !h->grid.slabs && h->p[0] == h->p[1] && h->p[1] == h->p[2] && h->p[0] <= 3;
+  return h->cfg.kernel_path != FVH_PATH_GENERIC && h->ndim == 3 && h->nv == 5 && !h->grid.slabs &&
+         h->p[0] == h->p[1] && h->p[1] == h->p[2] && h->p[0] <= 3;
 }
 
 template <typename Tc>
 struct Stream3Tiles;
 template <>
 struct Stream3Tiles<float> {
-  static constexpr int OY = 8, OZ = 32;
+  static constexpr int OY = 8, OZ = 32, NT = 256;
 };
 template <>
 struct Stream3Tiles<double> {
-  static constexpr int OY = 8, OZ = 16;
+  static constexpr int OY = 8, OZ = 16, NT = 256;
 };
 
 template <typename Tc, int P, bool REDUCE>
 int stream3d_p(fvh_handle* h, const double* state, int g, Tc* dst, const ReduceSpec& rs, cudaStream_t s) {
   using T = Stream3Tiles<Tc>;
   constexpr int KC = 2 * (P / 2) + 1;
-  using D = s3::Stream3Dims<Tc, P, T::OY, T::OZ>;
-  auto kern = s3::k3s_primitives<Tc, P, T::OY, T::OZ, KC, REDUCE>;
+  using D = s3::Stream3Dims<Tc, P, T::OY, T::OZ, T::NT>;
+  auto kern = s3::k3s_primitives<Tc, P, T::OY, T::OZ, T::NT, KC, REDUCE>;
   cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, D::BYTES);
   const Region rW = padded_region(h, g);
   const int ty = (rW.n[1] + T::OY - 1) / T::OY, tz = (rW.n[2] + T::OZ - 1) / T::OZ;
   // enough x chunks for about four waves of blocks; each chunk re-reads 3 RC planes
   int blocks_per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, (const void*)kern, 256, D::BYTES);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, (const void*)kern, T::NT, D::BYTES);
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->cfg.device);
   const int want = std::max(1, 4 * sms * std::max(blocks_per_sm, 1) / (ty * tz));
@@ -460,7 +457,7 @@ int stream3d_p(fvh_handle* h, const double* state, int g, Tc* dst, const ReduceS
   const dim3 grid(tz, ty, (rW.n[0] + chunk - 1) / chunk);
   const double pts = (double)region_points(rW);
   LaunchScope scope(KK_CENTRE, (double)h->n[0] * h->n[1] * h->n[2] * 5 * 8.0 + pts * 5 * sizeof(Tc), s);
-  kern<<<grid, 256, D::BYTES, s>>>(state, h->grid, make_view(dst, rW), g, chunk, device_rule<Tc, KC>(centre_rule(P)),
+  kern<<<grid, T::NT, D::BYTES, s>>>(state, h->grid, make_view(dst, rW), g, chunk, device_rule<Tc, KC>(centre_rule(P)),
                                    device_rule<Tc, KC>(transverse_rule(P)), make_phys<Tc>(h), rs, h->sc);
   return set_cuda_error(h, "streaming 3D primitives");
 }
@@ -496,7 +493,7 @@ int run_stage_t(fvh_handle* h, const StageCall& c, cudaStream_t s) {
   rs.ext_box = padded_region(h, 3);
   rs.ndim = (double)h->ndim;
   const Region rW = padded_region(h, h->gW);
-  const bool stream3 = stream3d_eligible<Tc>(h);
+  const bool stream3 = stream3d_eligible(h);
   if (stream3) {
     if ((st = stream3d<Tc, true>(h, c.stage_in, h->gW, (Tc*)h->W, rs, s))) return st;
   } else if ((st = primitive_pass<Tc, NV>(h, c.stage_in, h->gW, (Tc*)h->W, rs, true, true, s))) {

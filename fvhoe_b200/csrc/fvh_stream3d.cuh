@@ -14,6 +14,8 @@
 //   C(i) = C_z C_y C_x u at plane i (RC = p / 2, the centre rule's radius),
 //   converted to primitives, into a ring of 2RC+1 planes;
 //   W(i-RC) = T_z T_y T_x of the primitive ring, written to global memory.
+// The sweeps along x and y run on whole 16-byte vectors along z (rows of the
+// tiles are padded to whole vectors), the sweeps along z one point at a time.
 // Every sum runs from tap 0 upwards in the generic path's axis order, and the
 // ghost cells come through the same ghost maps (fvhoe/boundary_conditions.py:
 // 60-151) with the reflective sign applied to the FP64 value before the
@@ -26,24 +28,31 @@
 namespace fvh {
 namespace s3 {
 
-template <typename Tc, int P, int OY, int OZ>
+template <typename Tc, int P, int OY, int OZ, int NT = 256>
 struct Stream3Dims {
+  static constexpr int VW = 16 / (int)sizeof(Tc);  // elements per 16-byte shared-memory vector
   static constexpr int RC = P / 2;
   static constexpr int LY = OY + 4 * RC, LZ = OZ + 4 * RC;  // state plane tile
   static constexpr int CY = OY + 2 * RC, CZ = OZ + 2 * RC;  // after the centre sweeps
-  static constexpr int NU = 2 * RC + 1;                     // state ring (the centre rule's planes)
-  static constexpr int NP = 2 * RC + 1;                     // primitive ring
-  static constexpr int PL = LY * LZ, PC = CY * CZ;
-  // bytes: state ring (compute type), x-swept plane A (5 LY LZ), y-swept plane B
-  // (5 CY LZ), primitive ring (NP x 5 CY CZ), offsets and flip bits of the
-  // plane tile's y-z points
-  static constexpr int U_BYTES = NU * 5 * PL * (int)sizeof(Tc);
-  static constexpr int LOADS = (5 * PL + 255) / 256;  // state values a thread stages per plane
-  static constexpr int A_ELEMS = 5 * PL, B_ELEMS = 5 * CY * LZ, R_ELEMS = NP * 5 * PC;
-  static constexpr int BYTES = U_BYTES + (A_ELEMS + B_ELEMS + R_ELEMS) * (int)sizeof(Tc) + PL * 4 + PL + 16;
-  // resident blocks the shared memory allows (at most three), for the launch bounds
+  static constexpr int CZS = (CZ + VW - 1) / VW * VW;       // primitive rows padded to whole vectors
+  static_assert(OZ % VW == 0 && LZ % VW == 0, "tile rows must hold whole vectors");
+  static constexpr int NU = 2 * RC + 1;  // state ring (the centre rule's planes)
+  static constexpr int NP = 2 * RC + 1;  // primitive ring
+  static constexpr int PL = LY * LZ, PCS = CY * CZS;
+  // shared memory, in elements of the compute type: the state ring (NU x 5 x
+  // PL); A, the x-swept plane (5 x LY x LZ), later the x-transverse plane
+  // (5 x CY x CZS); B, the y-swept plane (5 x CY x LZ), later the y-transverse
+  // plane (5 x OY x CZS); the primitive ring (NP x 5 x CY x CZS); then the
+  // offsets and flip bits of the plane tile's y-z points
+  static constexpr int U_ELEMS = NU * 5 * PL, A_ELEMS = 5 * PL, B_ELEMS = 5 * CY * LZ, R_ELEMS = NP * 5 * PCS;
+  static_assert(5 * CY * CZS <= A_ELEMS && 5 * OY * CZS <= B_ELEMS, "transverse planes fit the swept ones");
+  static constexpr int LOADS = (5 * PL + NT - 1) / NT;  // state values a thread stages per plane
+  static constexpr int BYTES = (U_ELEMS + A_ELEMS + B_ELEMS + R_ELEMS) * (int)sizeof(Tc) + PL * 4 + PL + 16;
+  // resident blocks the shared memory allows (at most 768 threads per SM), for
+  // the launch bounds
   static constexpr int FIT = (228 * 1024) / (BYTES + 1024);
-  static constexpr int BLOCKS = FIT < 1 ? 1 : (FIT > 3 ? 3 : FIT);
+  static constexpr int CAP = 768 / NT;
+  static constexpr int BLOCKS = FIT < 1 ? 1 : (FIT > CAP ? CAP : FIT);
 };
 
 __device__ __forceinline__ int ring(int i, int n) {
@@ -55,16 +64,16 @@ __device__ __forceinline__ int ring(int i, int n) {
 // W over [-g, n+g)^3 for a block's y-z tile (blockIdx.x along z, blockIdx.y
 // along y) and its chunk of output planes along x (blockIdx.z). REDUCE: the
 // CFL maximum over rs.cfl_box and the per-variable extrema over rs.ext_box.
-template <typename Tc, int P, int OY, int OZ, int KC, bool REDUCE>
-__global__ void __launch_bounds__(256, (Stream3Dims<Tc, P, OY, OZ>::BLOCKS))
+template <typename Tc, int P, int OY, int OZ, int NT, int KC, bool REDUCE>
+__global__ void __launch_bounds__(NT, (Stream3Dims<Tc, P, OY, OZ, NT>::BLOCKS))
     k3s_primitives(const double* __restrict__ u, Grid grid, View<Tc> W, int g, int chunk, Rule<Tc, KC> c,
                    Rule<Tc, KC> t, Phys<Tc> ph, ReduceSpec rs, Scalars* __restrict__ sc) {
-  using D = Stream3Dims<Tc, P, OY, OZ>;
-  constexpr int RC = D::RC, LZ = D::LZ, CY = D::CY, CZ = D::CZ, PL = D::PL, PC = D::PC, NU = D::NU,
-                NP = D::NP;
+  using D = Stream3Dims<Tc, P, OY, OZ, NT>;
+  constexpr int RC = D::RC, LY = D::LY, LZ = D::LZ, CY = D::CY, CZ = D::CZ, CZS = D::CZS, PL = D::PL,
+                PCS = D::PCS, NU = D::NU, NP = D::NP, VW = D::VW;
   extern __shared__ __align__(16) unsigned char smem[];
   Tc* const U = reinterpret_cast<Tc*>(smem);  // NU x 5 x PL: state planes, sign-corrected, converted
-  Tc* const A = reinterpret_cast<Tc*>(smem + D::U_BYTES);
+  Tc* const A = U + D::U_ELEMS;
   Tc* const B = A + D::A_ELEMS;
   Tc* const R = B + D::B_ELEMS;
   int* const off = reinterpret_cast<int*>(R + D::R_ELEMS);              // y-z source offset of each plane point
@@ -77,7 +86,7 @@ __global__ void __launch_bounds__(256, (Stream3Dims<Tc, P, OY, OZ>::BLOCKS))
   const int xe = min(xb + chunk, n0 + g);
   // ghost maps of the tile's y-z points (the same for every plane); points
   // past the deepest ghost cell any output needs are clamped (they feed none)
-  for (int e = threadIdx.x; e < PL; e += blockDim.x) {
+  for (int e = threadIdx.x; e < PL; e += NT) {
     const int r = e / LZ, q = e - r * LZ;
     const int yi = min(max(y0 - 2 * RC + r, -gmax), n1 + gmax - 1);
     const int zi = min(max(z0 - 2 * RC + q, -gmax), n2 + gmax - 1);
@@ -100,7 +109,7 @@ __global__ void __launch_bounds__(256, (Stream3Dims<Tc, P, OY, OZ>::BLOCKS))
     const double* src = u + (size_t)jx * n1 * n2;
 #pragma unroll
     for (int m = 0; m < D::LOADS; ++m) {
-      const int idx = threadIdx.x + 256 * m;
+      const int idx = threadIdx.x + NT * m;
       if (idx < 5 * PL) {
         const int v = idx / PL, e = idx - v * PL;
         stage[m] = src[(size_t)v * plane + off[e]];
@@ -111,7 +120,7 @@ __global__ void __launch_bounds__(256, (Stream3Dims<Tc, P, OY, OZ>::BLOCKS))
     Tc* dst = U + ring(xi, NU) * 5 * PL;
 #pragma unroll
     for (int m = 0; m < D::LOADS; ++m) {
-      const int idx = threadIdx.x + 256 * m;
+      const int idx = threadIdx.x + NT * m;
       if (idx < 5 * PL) {
         const int v = idx / PL, e = idx - v * PL;
         double d = stage[m];
@@ -134,36 +143,61 @@ __global__ void __launch_bounds__(256, (Stream3Dims<Tc, P, OY, OZ>::BLOCKS))
     __syncthreads();  // state planes i-RC .. i+RC are in the ring
     const bool ahead = i + RC + 1 <= xe - 1 + 2 * RC;
     if (ahead) fetch(i + RC + 1);  // in flight while this plane is computed
-    // centre sweep along x
-    for (int idx = threadIdx.x; idx < 5 * PL; idx += blockDim.x) {
-      Tc acc = Tc(0);
+    // centre sweep along x: A = sum_k c_k U(i-RC+k), whole vectors of the plane
+    {
+      int sk[KC];
 #pragma unroll
-      for (int k = 0; k < KC; ++k) acc = acc + c.w[k] * U[ring(i - RC + k, NU) * 5 * PL + idx];
-      A[idx] = acc;
+      for (int k = 0; k < KC; ++k) sk[k] = ring(i - RC + k, NU) * 5 * PL;
+      for (int iv = threadIdx.x; iv < 5 * PL / VW; iv += NT) {
+        Tc acc[VW];
+#pragma unroll
+        for (int j = 0; j < VW; ++j) acc[j] = Tc(0);
+#pragma unroll
+        for (int k = 0; k < KC; ++k) {
+          Tc x[VW];
+          f2::ldn<VW>(U + sk[k] + iv * VW, x);
+#pragma unroll
+          for (int j = 0; j < VW; ++j) acc[j] = acc[j] + c.w[k] * x[j];
+        }
+        f2::stn<VW>(A + iv * VW, acc);
+      }
     }
     __syncthreads();
     // plane i+RC+1 into the slot of plane i-RC, which the centre sweep above
     // was the last to read (the next iteration's first barrier orders it)
     if (ahead) store(i + RC + 1);
-    // centre sweep along y: B (5 x CY x LZ)
-    for (int idx = threadIdx.x; idx < 5 * CY * LZ; idx += blockDim.x) {
-      const int v = idx / (CY * LZ), rem = idx - v * (CY * LZ), y = rem / LZ, z = rem - y * LZ;
-      const Tc* p = A + v * PL + y * LZ + z;
-      Tc acc = Tc(0);
+    // centre sweep along y: B (5 x CY x LZ), whole vectors along z
+    {
+      constexpr int LZV = LZ / VW;
+      for (int it = threadIdx.x; it < 5 * CY * LZV; it += NT) {
+        const int r = it / LZV, zq = it - r * LZV;
+        const int v = r / CY, y = r - v * CY;
+        const Tc* p = A + (v * LY + y) * LZ + zq * VW;
+        Tc acc[VW];
 #pragma unroll
-      for (int k = 0; k < KC; ++k) acc = acc + c.w[k] * p[k * LZ];
-      B[idx] = acc;
+        for (int j = 0; j < VW; ++j) acc[j] = Tc(0);
+#pragma unroll
+        for (int k = 0; k < KC; ++k) {
+          Tc x[VW];
+          f2::ldn<VW>(p + k * LZ, x);
+#pragma unroll
+          for (int j = 0; j < VW; ++j) acc[j] = acc[j] + c.w[k] * x[j];
+        }
+        f2::stn<VW>(B + r * LZ + zq * VW, acc);
+      }
     }
     __syncthreads();
-    // centre sweep along z and the conversion: primitive plane i into its ring slot
+    // centre sweep along z and the conversion: primitive plane i into its ring
+    // slot (rows of CZS; the padding columns are never written and feed only
+    // padding outputs)
     {
-      Tc* Ri = R + ring(i, NP) * 5 * PC;
-      for (int idx = threadIdx.x; idx < PC; idx += blockDim.x) {
+      Tc* Ri = R + ring(i, NP) * 5 * PCS;
+      for (int idx = threadIdx.x; idx < CY * CZ; idx += NT) {
         const int y = idx / CZ, z = idx - y * CZ;
         Tc uc[5], w[5];
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-          const Tc* p = B + v * (CY * LZ) + y * LZ + z;
+          const Tc* p = B + (v * CY + y) * LZ + z;
           Tc acc = Tc(0);
 #pragma unroll
           for (int k = 0; k < KC; ++k) acc = acc + c.w[k] * p[k];
@@ -171,39 +205,62 @@ __global__ void __launch_bounds__(256, (Stream3Dims<Tc, P, OY, OZ>::BLOCKS))
         }
         to_primitives(ph, 5, uc, w);
 #pragma unroll
-        for (int v = 0; v < 5; ++v) Ri[v * PC + idx] = w[v];
+        for (int v = 0; v < 5; ++v) Ri[(v * CY + y) * CZS + z] = w[v];
       }
     }
     __syncthreads();
     const int xo = i - RC;
     if (xo < xb) continue;
-    // transverse sweep along x over the primitive ring: A (5 x CY x CZ)
-    for (int idx = threadIdx.x; idx < 5 * PC; idx += blockDim.x) {
-      Tc acc = Tc(0);
+    // transverse sweep along x over the primitive ring: A (5 x CY x CZS)
+    {
+      int rk[KC];
 #pragma unroll
-      for (int k = 0; k < KC; ++k) acc = acc + t.w[k] * R[ring(xo - RC + k, NP) * 5 * PC + idx];
-      A[idx] = acc;
+      for (int k = 0; k < KC; ++k) rk[k] = ring(xo - RC + k, NP) * 5 * PCS;
+      for (int iv = threadIdx.x; iv < 5 * PCS / VW; iv += NT) {
+        Tc acc[VW];
+#pragma unroll
+        for (int j = 0; j < VW; ++j) acc[j] = Tc(0);
+#pragma unroll
+        for (int k = 0; k < KC; ++k) {
+          Tc x[VW];
+          f2::ldn<VW>(R + rk[k] + iv * VW, x);
+#pragma unroll
+          for (int j = 0; j < VW; ++j) acc[j] = acc[j] + t.w[k] * x[j];
+        }
+        f2::stn<VW>(A + iv * VW, acc);
+      }
     }
     __syncthreads();
-    // transverse sweep along y: B (5 x OY x CZ)
-    for (int idx = threadIdx.x; idx < 5 * OY * CZ; idx += blockDim.x) {
-      const int v = idx / (OY * CZ), rem = idx - v * (OY * CZ), y = rem / CZ, z = rem - y * CZ;
-      const Tc* p = A + v * PC + y * CZ + z;
-      Tc acc = Tc(0);
+    // transverse sweep along y: B (5 x OY x CZS), whole vectors along z
+    {
+      constexpr int CZV = CZS / VW;
+      for (int it = threadIdx.x; it < 5 * OY * CZV; it += NT) {
+        const int r = it / CZV, zq = it - r * CZV;
+        const int v = r / OY, y = r - v * OY;
+        const Tc* p = A + (v * CY + y) * CZS + zq * VW;
+        Tc acc[VW];
 #pragma unroll
-      for (int k = 0; k < KC; ++k) acc = acc + t.w[k] * p[k * CZ];
-      B[idx] = acc;
+        for (int j = 0; j < VW; ++j) acc[j] = Tc(0);
+#pragma unroll
+        for (int k = 0; k < KC; ++k) {
+          Tc x[VW];
+          f2::ldn<VW>(p + k * CZS, x);
+#pragma unroll
+          for (int j = 0; j < VW; ++j) acc[j] = acc[j] + t.w[k] * x[j];
+        }
+        f2::stn<VW>(B + r * CZS + zq * VW, acc);
+      }
     }
     __syncthreads();
     // transverse sweep along z: W at output plane xo, and the reductions
-    for (int idx = threadIdx.x; idx < OY * OZ; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < OY * OZ; idx += NT) {
       const int y = idx / OZ, z = idx - y * OZ;
       const int yi = y0 + y, zi = z0 + z;
       if (yi >= n1 + g || zi >= n2 + g) continue;
       Tc w[5];
 #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        const Tc* p = B + v * (OY * CZ) + y * CZ + z;
+        const Tc* p = B + (v * OY + y) * CZS + z;
         Tc acc = Tc(0);
 #pragma unroll
         for (int k = 0; k < KC; ++k) acc = acc + t.w[k] * p[k];

@@ -315,11 +315,11 @@ def test_host_state_steps_equal_device_steps(precision):
 @pytest.mark.parametrize("p", [0, 1, 2, 3])
 @pytest.mark.parametrize("n", [(20, 18, 17), (33, 16, 41)])
 def test_streaming_3d_primitives_equal_generic(p, n, precision):
-    """3D problems ("auto") detect troubled cells with the sliding-window
-    kernel, and in FP32 with p <= 3 run their primitive passes as one
-    streaming kernel; the steps equal the generic kernels' bit for bit on
-    ragged grids (chunks along x cut short) with mixed periodic, outflow and
-    reflective sides."""
+    """3D problems ("auto") with p <= 3 run their primitive passes as one
+    streaming kernel, detect troubled cells with the sliding-window kernel and
+    solve the fallback from compacted face lists; the steps equal the generic
+    kernels' bit for bit on ragged grids (chunks along x cut short, tiles past
+    the box) with mixed periodic, outflow and reflective sides."""
     from fvhoe_b200 import BoundaryCondition, EulerSolver, SedovBlast
 
     kw = dict(w0=SedovBlast(dims="xyz"), conservative_ic=True, fv_ic=True, nx=n[0], ny=n[1], nz=n[2], px=p, py=p,
