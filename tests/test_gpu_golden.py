@@ -333,3 +333,41 @@ def test_streaming_3d_primitives_equal_generic(p, n, precision):
     assert stream.t == generic.t
     assert np.array_equal(stream.am.get_numpy("u"), generic.am.get_numpy("u"))
     assert np.array_equal(stream.trouble_flags(), generic.trouble_flags())
+
+
+_MODES_3D = {
+    "local_relative": dict(NAD_mode="local", NAD_range="relative"),
+    "global_absolute_nosed": dict(NAD_mode="global", NAD_range="absolute", SED=False),
+    "local_absolute_vars": dict(NAD_mode="local", NAD_range="absolute", NAD_vars=("rho", "P")),
+    "moncen": dict(slope_limiter="moncen"),
+    "unlimited": dict(slope_limiter=None),
+    "passives": dict(w0_passives={"tracer": lambda x, y, z: np.sin(6.0 * x) * np.cos(4.0 * z)}),
+}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("mode", list(_MODES_3D))
+def test_3d_detection_and_fallback_modes_equal_generic(mode, precision):
+    """The sliding-window 3D detection, the compacting fallback and (five
+    variables) the streaming primitive pass against the generic kernels under
+    the detector's modes: local and absolute NAD ranges, SED off, a variable
+    subset, the moncen and unlimited fallbacks, and passive scalars (which take
+    the variable-count-at-run-time kernels); bit for bit, flags and logs too."""
+    from fvhoe_b200 import BoundaryCondition, EulerSolver, SedovBlast
+
+    kw = dict(w0=SedovBlast(dims="xyz"), conservative_ic=True, fv_ic=True, nx=19, ny=22, nz=17, px=2, py=2, pz=2,
+              gamma=1.4, riemann_solver="hllc", CFL=0.5, precision=precision,
+              bc=BoundaryCondition(x=("reflective", "outflow"), y=("outflow", "reflective"),
+                                   z=("outflow", "reflective")),
+              a_posteriori_slope_limiting=True, NAD=1e-4, progress_bar=False)
+    kw.update(_MODES_3D[mode])
+    fast = EulerSolver(kernel_path="auto", **kw)
+    generic = EulerSolver(kernel_path="generic", **kw)
+    fast.ssprk3(n=3)
+    generic.ssprk3(n=3)
+    assert fast.t == generic.t
+    assert np.array_equal(fast.am.get_numpy("u"), generic.am.get_numpy("u"))
+    assert np.array_equal(fast.trouble_flags(), generic.trouble_flags())
+    for a, b in zip(fast._trouble_logs(), generic._trouble_logs()):
+        assert np.array_equal(a, b)
