@@ -289,4 +289,87 @@ __global__ void __launch_bounds__(NT, (Stream3Dims<Tc, P, OY, OZ, NT>::BLOCKS))
 }
 
 }  // namespace s3
+// ---------------------------------------------------------------------------
+// Two consecutive sweeps of five variables in one launch: out = S2(S1(in)),
+// S1 along axis A1 with rule r1 (K1 taps), S2 along A2 with r2 (K2 taps),
+// every sum from tap 0 upwards and the intermediate rounded to Tc, as two
+// sweep launches with a stored intermediate compute them. A block owns a tile
+// of T0 x T1 x T2 outputs (axis 2 contiguous, no halo on the unswept axis):
+// it loads the input tile with its halos, sweeps it along A1 into a second
+// shared tile and sweeps that along A2 into the output, one point per thread
+// and pass. Input points past the input region (only partial tiles reach
+// them) are clamped into it; they feed only outputs past the box, which are
+// not stored.
+// ---------------------------------------------------------------------------
+template <int A1, int A2, int K1, int K2, int T0, int T1, int T2>
+struct PairDims {
+  static constexpr int N0 = T0 + (A1 == 0 ? K1 - 1 : 0) + (A2 == 0 ? K2 - 1 : 0);
+  static constexpr int N1 = T1 + (A1 == 1 ? K1 - 1 : 0) + (A2 == 1 ? K2 - 1 : 0);
+  static constexpr int N2 = T2 + (A1 == 2 ? K1 - 1 : 0) + (A2 == 2 ? K2 - 1 : 0);
+  static constexpr int M0 = T0 + (A2 == 0 ? K2 - 1 : 0);  // after the first sweep
+  static constexpr int M1 = T1 + (A2 == 1 ? K2 - 1 : 0);
+  static constexpr int M2 = T2 + (A2 == 2 ? K2 - 1 : 0);
+  static constexpr int NP = N0 * N1 * N2, MP = M0 * M1 * M2;
+  template <typename Tc>
+  static constexpr int bytes() {
+    return 5 * (NP + MP) * (int)sizeof(Tc);
+  }
+};
+
+template <typename Tc, int A1, int A2, int K1, int K2, int T0, int T1, int T2, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+    k_sweep_pair(View<const Tc> in, Region rin, View<Tc> out, Box box, Rule<Tc, K1> r1, Rule<Tc, K2> r2) {
+  static_assert(A1 != A2, "two different axes");
+  using D = PairDims<A1, A2, K1, K2, T0, T1, T2>;
+  constexpr int N1 = D::N1, N2 = D::N2, M1 = D::M1, M2 = D::M2;
+  extern __shared__ __align__(16) unsigned char pair_smem[];
+  Tc* const S = reinterpret_cast<Tc*>(pair_smem);  // 5 x N0 x N1 x N2
+  Tc* const Mid = S + 5 * D::NP;                   // 5 x M0 x M1 x M2
+  const int o0 = box.lo[0] + (int)blockIdx.z * T0, o1 = box.lo[1] + (int)blockIdx.y * T1,
+            o2 = box.lo[2] + (int)blockIdx.x * T2;
+  // input origin: the output origin moved by each sweep's first tap
+  const int i0 = o0 + (A1 == 0 ? r1.off : 0) + (A2 == 0 ? r2.off : 0);
+  const int i1 = o1 + (A1 == 1 ? r1.off : 0) + (A2 == 1 ? r2.off : 0);
+  const int i2 = o2 + (A1 == 2 ? r1.off : 0) + (A2 == 2 ? r2.off : 0);
+  for (int idx = threadIdx.x; idx < D::NP; idx += 256) {
+    const int p0 = idx / (N1 * N2), rem = idx - p0 * (N1 * N2), p1 = rem / N2, p2 = rem - p1 * N2;
+    const int g0 = min(i0 + p0, rin.lo[0] + rin.n[0] - 1), g1 = min(i1 + p1, rin.lo[1] + rin.n[1] - 1),
+              g2 = min(i2 + p2, rin.lo[2] + rin.n[2] - 1);
+    const Tc* q = in.p + in.at(g0, g1, g2);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) S[v * D::NP + idx] = q[v * in.vs];
+  }
+  __syncthreads();
+  constexpr int SA1 = A1 == 0 ? N1 * N2 : (A1 == 1 ? N2 : 1);  // stride of A1 in S
+  for (int idx = threadIdx.x; idx < D::MP; idx += 256) {
+    const int m0 = idx / (M1 * M2), rem = idx - m0 * (M1 * M2), m1 = rem / M2, m2 = rem - m1 * M2;
+    const int src = (m0 * N1 + m1) * N2 + m2;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const Tc* q = S + v * D::NP + src;
+      Tc acc = Tc(0);
+#pragma unroll
+      for (int k = 0; k < K1; ++k) acc = acc + r1.w[k] * q[k * SA1];
+      Mid[v * D::MP + idx] = acc;
+    }
+  }
+  __syncthreads();
+  constexpr int SA2 = A2 == 0 ? M1 * M2 : (A2 == 1 ? M2 : 1);  // stride of A2 in Mid
+  for (int idx = threadIdx.x; idx < T0 * T1 * T2; idx += 256) {
+    const int t0 = idx / (T1 * T2), rem = idx - t0 * (T1 * T2), t1 = rem / T2, t2 = rem - t1 * T2;
+    const int x0 = o0 + t0, x1 = o1 + t1, x2 = o2 + t2;
+    if (x0 >= box.lo[0] + box.n[0] || x1 >= box.lo[1] + box.n[1] || x2 >= box.lo[2] + box.n[2]) continue;
+    const int src = (t0 * M1 + t1) * M2 + t2;
+    Tc* o = out.p + out.at(x0, x1, x2);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const Tc* q = Mid + v * D::MP + src;
+      Tc acc = Tc(0);
+#pragma unroll
+      for (int k = 0; k < K2; ++k) acc = acc + r2.w[k] * q[k * SA2];
+      o[v * out.vs] = acc;
+    }
+  }
+}
+
 }  // namespace fvh
