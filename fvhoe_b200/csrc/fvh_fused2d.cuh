@@ -359,10 +359,15 @@ struct PrimsDims {
   static constexpr int PY = OY + 2 * RC;                    // after the Y centre sweep: CX x PY
   static constexpr int LYS = (LY + VW - 1) / VW * VW, PYS = (PY + VW - 1) / VW * VW, OYS = (OY + VW - 1) / VW * VW;
   static constexpr int PAD = 16;
-  // A: after the Y centre sweep CX x PY, after the Y transverse sweep OX x OY;
-  // B: after the X centre sweep CX x LY, after the X transverse sweep OX x PY
-  // (the loaded state is never stored: its columns are swept as they arrive)
-  static constexpr int A = Max<CX * PYS, OX * OYS>::value * 5 + PAD;
+  // WALK (rules of 5 or more taps, p >= 4): the loaded state is never stored,
+  // its columns are swept along X as they arrive; with 3-tap rules the state
+  // tile is staged in A first (measured faster there: the column walks leave
+  // each thread a long chain of loads for little saved shared-memory work).
+  static constexpr bool WALK = 2 * RC + 1 >= 5;
+  // A: the staged state LX x LY (without WALK), after the Y centre sweep
+  // CX x PY, after the Y transverse sweep OX x OY; B: after the X centre sweep
+  // CX x LY, after the X transverse sweep OX x PY
+  static constexpr int A = Max<Max<(WALK ? 0 : LX * LYS), CX * PYS>::value, OX * OYS>::value * 5 + PAD;
   static constexpr int B = Max<CX * LYS, OX * PYS>::value * 5 + PAD;
   // row segments per column in the X centre sweep: enough column segments
   // (five variables per column) for one per thread of a 256-thread block
@@ -427,16 +432,68 @@ __device__ __forceinline__ void primitives_tile(const Tin* __restrict__ u, const
   using D = PrimsDims<Tc, P, OX, OY>;
   constexpr int RC = D::RC, VW = VecW<Tc>::value;
   const int nt = blockDim.x;
-  // 1. the state with 2*RC ghosts around the tile, swept along X as its
-  // columns arrive: B, CX x LYS. A tile whose loaded box lies inside the grid
-  // (most tiles) reads the state directly; the others resolve every point
-  // through the ghost maps.
+  // 1. the state with 2*RC ghosts around the tile, swept along X: B, CX x
+  // LYS; staged in A first (3-tap rules) or swept as its columns arrive
+  // (WALK). A tile whose loaded box lies inside the grid (most tiles) reads
+  // the state directly; the others resolve every point through the ghost maps.
   const int lx0 = x0 - 2 * RC, ly0 = y0 - 2 * RC;
-  if (!g.slabs && lx0 >= 0 && lx0 + D::LX <= g.nx && ly0 >= 0 && ly0 + D::LY <= g.ny) {
+  const bool inside = !g.slabs && lx0 >= 0 && lx0 + D::LX <= g.nx && ly0 >= 0 && ly0 + D::LY <= g.ny;
+  if constexpr (!D::WALK) {
+    // the state tile staged in A (LX x LYS), then the X centre sweep into B
+    if (inside) {
+      const int plane = g.nx * g.ny;
+      for (int i = threadIdx.x; i < D::LX * D::LY; i += nt) {
+        const int r = i / D::LY, q = i - r * D::LY;
+        const Tin* p = u + (lx0 + r) * g.ny + ly0 + q;
+        Tin sv[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) sv[v] = p[v * plane];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) A[(v * D::LX + r) * D::LYS + q] = (Tc)sv[v];
+      }
+    } else {
+      for (int i = threadIdx.x; i < D::LX * D::LY; i += nt) {
+        const int r = i / D::LY, q = i - r * D::LY;
+        Tc sv[5];
+        load_state2<Tc>(u, g, lx0 + r, ly0 + q, sv);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) A[(v * D::LX + r) * D::LYS + q] = sv[v];
+      }
+    }
+    __syncthreads();
+    sweepv<Tc, VW, KC, 1, 0, D::CX, D::LYS / VW, D::LYS, D::LX * D::LYS, D::A, mrow_prims<Tc>()>(
+        A, c.w, [&](int v, int r, int q, const Tc* acc) { stn<VW>(B + (v * D::CX + r) * D::LYS + q, acc); });
+  } else if (inside) {
     const int plane = g.nx * g.ny;
     const Tin* base = u + lx0 * g.ny + ly0;
     centre_x_columns<Tc, KC, D::CX, D::LY, D::LYS, D::NS>(
         B, c.w, [&](int r, int q, int v) { return (Tc)base[v * plane + r * g.ny + q]; });
+  } else if (!g.slabs) {
+    // the ghost maps are separable: each tile row's and column's source
+    // index and mirror flag (j << 1 | flip), resolved once into A (free until
+    // the Y centre sweep), as load_state2 resolves them point by point
+    int* const mx = reinterpret_cast<int*>(A);
+    int* const my = mx + D::LX;
+    for (int i = threadIdx.x; i < D::LX + D::LY; i += nt) {
+      bool f = false;
+      if (i < D::LX) {
+        const int x = min(max(lx0 + i, -g.gmax), g.nx + g.gmax - 1);
+        const int j = ghost_source(x, g.nx, g.bcx[0], g.bcx[1], f);
+        mx[i] = (j << 1) | (f ? 1 : 0);
+      } else {
+        const int y = min(max(ly0 + i - D::LX, -g.gmax), g.ny + g.gmax - 1);
+        const int j = ghost_source(y, g.ny, g.bcy[0], g.bcy[1], f);
+        my[i - D::LX] = (j << 1) | (f ? 1 : 0);
+      }
+    }
+    __syncthreads();
+    const int plane = g.nx * g.ny;
+    centre_x_columns<Tc, KC, D::CX, D::LY, D::LYS, D::NS>(B, c.w, [&](int r, int q, int v) {
+      const int a = mx[r], b = my[q];
+      double val = (double)u[v * plane + (a >> 1) * g.ny + (b >> 1)];
+      if ((v == 1 + g.dx && (a & 1)) || (v == 1 + g.dy && (b & 1))) val = -val;
+      return (Tc)val;
+    });
   } else {
     centre_x_columns<Tc, KC, D::CX, D::LY, D::LYS, D::NS>(
         B, c.w, [&](int r, int q, int v) { return load_var2<Tc>(u, g, lx0 + r, ly0 + q, v); });
