@@ -82,8 +82,8 @@ def workload_config(args, n=None):
         "riemann": "hllc",
         "integrator": "ssprk3",
         "precision": args.precision,
-        "step": "one SSP-RK3 step = 3 stages = 3 cell-updates per cell",
-        "l2": "inputs larger than L2: the float64 state alone is 5*8*n^2 bytes",
+        "step": "SSP-RK3 step: 3 cell-updates per cell",
+        "l2": "inputs larger than L2 (FP64 state 40 n^2 bytes)",
     }
 
 
@@ -718,8 +718,7 @@ def e2e_leg(lib, _capi, h, u, sp, stream, args, cells, world, dist):
     serial_s = max_over_ranks(time.perf_counter() - t0, dist)
     return {"value": world * 3 * cells * args.e2e_steps / e2e_s / 1e6, "unit": UNIT,
             "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": args.e2e_steps,
-            "path": "fvh_step_host through the C ABI: state in pinned host memory, copied in and out every "
-                    "step in 16 chunks on two copy streams",
+            "path": "fvh_step_host (C ABI), pinned host state copied in and out every step",
             "serial_value": world * 3 * cells * args.e2e_steps / serial_s / 1e6}
 
 
@@ -774,14 +773,14 @@ def accuracy_run(args, series, seed, stream):
 
 
 def leg_summary(legs):
-    """The few figures of each leg that the headline line repeats."""
+    """The few figures of each leg that the headline line repeats (the legs
+    are printed in full on their own lines before it)."""
     out = {}
     lp = legs.get("learned_predictor")
     if lp:
-        out["learned_predictor"] = ({k: lp[k] for k in ("config", "mcell_updates_per_s", "speedup_vs_plain_fp64")}
+        out["learned_predictor"] = ({k: {f: round(x, 3) for f, x in lp[k].items()}
+                                     for k in ("mcell_updates_per_s", "speedup_vs_plain_fp64")}
                                     if "error" not in lp else lp)
-        if "l1_density_error_vs_fp64" in lp:
-            out["learned_predictor"]["l1"] = lp["l1_density_error_vs_fp64"]
     sd = legs.get("sedov_3d")
     if sd:
         out["sedov_3d"] = ({k: sd[k]["mcell_updates_per_s"] for k in ("fp64", "fp32")} if "error" not in sd else sd)
@@ -791,6 +790,17 @@ def leg_summary(legs):
                                     "small_members_gain": be.get("small_members", {}).get("batching_gain")}
                                    if "error" not in be else be)
     return out
+
+
+def l1_summary(l1):
+    """The headline's L1 figures: the error at t_end, and per time of the series
+    [t, L1 of the chosen form, L1 of FP64 moved by one ulp (the chaos floor)]."""
+    if l1 is None:
+        return None
+    return {"t": l1["t"], "value": l1["value"],
+            "series": [[x["t"], x["l1"], x["l1_fp64_one_ulp"]] for x in l1["series"]],
+            "series_columns": ["t", "l1", "l1_fp64_one_ulp"],
+            "whole_run_speedup": l1["whole_run"]["speedup_of_chosen"]}
 
 
 def run_ours(args):
@@ -902,6 +912,8 @@ def run_ours(args):
             except Exception as exc:
                 legs["batched_ensemble"] = {"error": f"{type(exc).__name__}: {exc}"}
         # every leg in full on its own line, then the headline line last (compact)
+        if l1 is not None:
+            print("leg accuracy " + json.dumps(l1), flush=True)
         for name, leg in legs.items():
             print(f"leg {name} " + json.dumps(leg), flush=True)
         if kinds:
@@ -910,7 +922,7 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32", "data": "synthetic",
-            "plain_fp64": plain_line, "l1_density_error_vs_fp64": l1,
+            "plain_fp64": plain_line, "l1_density_error_vs_fp64": l1_summary(l1),
             "config": dict(workload_config(args), parallelism=f"replicas x{world}" if world > 1 else "single",
                            timed_from=f"t = {t_start} (both forms advanced there first)"),
             "chosen_form": form, "roofline": roofline, "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
