@@ -621,6 +621,15 @@ int step_stage(fvh_handle* h, double* u, int integrator, int k, int stages, doub
                double target, cudaStream_t s) {
   fvh::StageCall c{};
   const double* in = k == 0 ? u : h->S[(k - 1) & 1];
+  if (stages == 1) {
+    // A one-stage step writes u in place, while the final pass of a troubled
+    // tile reads its stage input in a halo of cells that neighbouring blocks
+    // update: the stage reads a copy of u instead.
+    const size_t bytes = (size_t)h->nv * h->n[0] * h->n[1] * h->n[2] * sizeof(double);
+    if (cudaMemcpyAsync(h->S[1], u, bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+      return fail(h, FVH_ERR_CUDA, std::string("stage input copy: ") + cudaGetErrorString(cudaGetLastError()));
+    in = h->S[1];
+  }
   c.stage_in = in;
   c.spec.integrator = integrator;  // FVH_INT_* and fvh::Integrator share values
   c.spec.stage = k;

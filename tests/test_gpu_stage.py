@@ -72,3 +72,30 @@ def test_stage_out_of_order_is_refused():
     assert lib.fvh_stage(a._handle, ua, ssprk3, 2, 0.0, 0, 0.0, None, stream) == _capi.ERR_ARG
     torch.cuda.synchronize()
     assert torch.equal(a.am("u"), before)  # stage 0 writes only the stage buffers
+
+
+@pytest.mark.parametrize("kernel_path", ["fused2d", "generic"])
+def test_euler_steps_equal_the_oracle(kernel_path, n=192, p=5, steps=3):
+    """A one-stage step updates u in place. The fused final pass of a troubled
+    tile reads the stage input two cells around the tile, cells that
+    neighbouring blocks update in the same launch, so the step must read a
+    copy of u: checked bit for bit against the oracle's forward Euler
+    (fvhoe/ode.py:245-252) on a grid of many troubled tiles."""
+    from fvhoe_b200 import ArrayIC, EulerSolver, KelvinHelmholtzNoise2D
+    from fvhoe_b200.solver import initial_state
+    from oracle import fvh_oracle as O
+
+    u = initial_state(KelvinHelmholtzNoise2D(n=(n, n), seed=4), n, n, 1, p, p, 0, gamma=1.4)
+    s = EulerSolver(w0=ArrayIC(array=u), conservative_ic=True, fv_ic=True, nx=n, ny=n, px=p, py=p, gamma=1.4,
+                    riemann_solver="hllc", CFL=0.8, a_posteriori_slope_limiting=True, NAD=1e-5,
+                    progress_bar=False, kernel_path=kernel_path)
+    cfg = O.OracleConfig(n=(n, n, 1), p=(p, p, 0), h=s.h, gamma=1.4, riemann_solver="hllc",
+                         a_posteriori_slope_limiting=True, NAD=1e-5)
+    t = 0.0
+    for _ in range(steps):
+        dt, u, _ = O.step(u, t, cfg, "euler")
+        t += dt
+    s.euler(n=steps)
+    assert s.t == t
+    assert int(s.trouble_flags().sum()) > 0
+    assert np.array_equal(s.am.get_numpy("u"), u)
