@@ -18,7 +18,10 @@
 //                  phase computes W* on each tile instead (tile2_detect)
 //   k2_final       MUSCL fallback fluxes at troubled faces, the blend, the flux
 //                  divergence and the Runge-Kutta combination
-//                  (fvhoe/solver.py:710-751, fvhoe/ode.py:245-298)
+//                  (fvhoe/solver.py:710-751, fvhoe/ode.py:245-298); in FP64
+//                  the fallback runs first in two launches of its own
+//                  (k2_face_list, k2_face_solve) and k2_final streams the
+//                  divergence and the combination alone
 // Shared-memory arrays are variable-major: element (v, r, c) of an R x C tile
 // sits at (v*R + r)*C + c.
 #pragma once
@@ -1212,10 +1215,13 @@ __global__ void __launch_bounds__(256, 6)
 // in flight together. SO: SSP-RK3 in the Shu-Osher form instead of the
 // reference's k-sum form (the FP32 form: the same scheme, FP64 rounding apart,
 // reading the stage input in place of the k-sum and writing no k-sum).
+// pa / pb (variable stride ps): the cell's a and b operands already staged in
+// shared memory, read there instead of from the arrays.
 // Returns how many results are not finite.
 template <int INTEG, int STAGE, bool SO = false>
 __device__ __forceinline__ unsigned int rk_combine(const StageSpec& st, int o, int plane, double dt,
-                                                   const double* k) {
+                                                   const double* k, const double* pa = nullptr,
+                                                   const double* pb = nullptr, int ps = 0) {
   double a[5], b[5], res[5];
   if constexpr (INTEG == INT_RHS) {
 #pragma unroll
@@ -1225,7 +1231,7 @@ __device__ __forceinline__ unsigned int rk_combine(const StageSpec& st, int o, i
     }
   } else if constexpr (INTEG == INT_EULER) {
 #pragma unroll
-    for (int v = 0; v < 5; ++v) a[v] = st.u[o + v * plane];
+    for (int v = 0; v < 5; ++v) a[v] = pa ? pa[v * ps] : st.u[o + v * plane];
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
       res[v] = a[v] + dt * k[v];
@@ -1234,8 +1240,8 @@ __device__ __forceinline__ unsigned int rk_combine(const StageSpec& st, int o, i
   } else if constexpr (INTEG == INT_SSPRK2) {
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
-      a[v] = st.u[o + v * plane];
-      if constexpr (STAGE != 0) b[v] = st.stage_in[o + v * plane];
+      a[v] = pa ? pa[v * ps] : st.u[o + v * plane];
+      if constexpr (STAGE != 0) b[v] = pb ? pb[v * ps] : st.stage_in[o + v * plane];
     }
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
@@ -1251,8 +1257,8 @@ __device__ __forceinline__ unsigned int rk_combine(const StageSpec& st, int o, i
     // u1 = u + dt k1; u2 = 3/4 u + 1/4 (u1 + dt k2); u3 = 1/3 u + 2/3 (u2 + dt k3)
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
-      a[v] = st.u[o + v * plane];
-      if constexpr (STAGE != 0) b[v] = st.stage_in[o + v * plane];
+      a[v] = pa ? pa[v * ps] : st.u[o + v * plane];
+      if constexpr (STAGE != 0) b[v] = pb ? pb[v * ps] : st.stage_in[o + v * plane];
     }
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
@@ -1271,8 +1277,8 @@ __device__ __forceinline__ unsigned int rk_combine(const StageSpec& st, int o, i
   } else if constexpr (INTEG == INT_SSPRK3) {
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
-      a[v] = st.u[o + v * plane];
-      if constexpr (STAGE != 0) b[v] = st.acc[o + v * plane];
+      a[v] = pa ? pa[v * ps] : st.u[o + v * plane];
+      if constexpr (STAGE != 0) b[v] = pb ? pb[v * ps] : st.acc[o + v * plane];
     }
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
@@ -1294,8 +1300,8 @@ __device__ __forceinline__ unsigned int rk_combine(const StageSpec& st, int o, i
   } else {  // INT_RK4
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
-      a[v] = st.u[o + v * plane];
-      if constexpr (STAGE != 0) b[v] = st.acc[o + v * plane];
+      a[v] = pa ? pa[v * ps] : st.u[o + v * plane];
+      if constexpr (STAGE != 0) b[v] = pb ? pb[v * ps] : st.acc[o + v * plane];
     }
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
@@ -1352,19 +1358,59 @@ struct FinalDims {
   // bytes after the three tiles: two counters and the compacted fallback face lists
   static constexpr int LIST = 16 + 2 * (NXF + NYF);
   static_assert(NXF < 65536 && NYF < 65536, "face indices are 16-bit");
+  // FP64 launches of a fixed integrator also stage the Runge-Kutta operands
+  // of the tile's cells (two FP64 arrays, 5 variables each), after the lists
+  static constexpr int LIST16 = (LIST + 15) / 16 * 16;
+  static constexpr int RKOP = 2 * 5 * TX * TY;
+  // FB: the fallback runs in the same launch (pointwise tile and face lists
+  // after the two flux tiles); without it the launch holds the flux tiles only
+  template <typename Tc>
+  static constexpr size_t rk_offset(bool fb) {
+    return fb ? (size_t)(SP + SF + SG) * sizeof(Tc) + LIST16 : ((size_t)(SF + SG) * sizeof(Tc) + 15) / 16 * 16;
+  }
+  template <typename Tc>
+  static constexpr size_t bytes(bool rk_operands, bool fb = true) {
+    return rk_operands ? rk_offset<Tc>(fb) + RKOP * sizeof(double)
+                       : (fb ? (size_t)(SP + SF + SG) * sizeof(Tc) + LIST : (size_t)(SF + SG) * sizeof(Tc));
+  }
 };
 
-// RKI < 0: the integrator and stage are read from st at run time.
-template <typename Tc, int TX, int TY, int RKI = -1, int RKS = 0>
+// The arrays the Runge-Kutta combination of INTEG / STAGE reads besides the
+// divergence (a: the step's initial state; b: the stage input or the k-sum;
+// nullptr where it reads none), as rk_combine reads them.
+template <int INTEG, int STAGE, bool SO>
+__device__ __forceinline__ void rk_sources(const StageSpec& st, const double*& a, const double*& b) {
+  a = INTEG == INT_RHS ? nullptr : st.u;
+  b = nullptr;
+  if constexpr (STAGE != 0) {
+    if constexpr (INTEG == INT_SSPRK2 || (INTEG == INT_SSPRK3 && SO)) {
+      b = st.stage_in;
+    } else if constexpr (INTEG == INT_SSPRK3 || INTEG == INT_RK4) {
+      b = st.acc;
+    }
+  }
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// RKI < 0: the integrator and stage are read from st at run time. FB: the
+// fallback fluxes of the tile's troubled faces are solved here (the batched
+// ensemble's phase); without it k2_face_solve has already written them into F
+// and G, and this is the divergence and the Runge-Kutta combination alone.
+template <typename Tc, int TX, int TY, int RKI = -1, int RKS = 0, bool FB = true>
 __device__ __forceinline__ void tile2_final(const double* __restrict__ stage_in, Geo g, V2<const Tc> F,
                                             V2<const Tc> G, const uint8_t* __restrict__ trouble,
                                             const uint8_t* __restrict__ pred, int apost, int muscl, int limiter,
                                             Phys<Tc> ph, double cx, double cy, StageSpec st, double dt_step,
                                             Scalars* __restrict__ sc, int bx, int by, unsigned char* smem_raw) {
   using D = FinalDims<TX, TY>;
-  Tc* Pw = reinterpret_cast<Tc*>(smem_raw);
-  Tc* FX = Pw + D::SP;
+  Tc* FX = reinterpret_cast<Tc*>(smem_raw);
   Tc* GY = FX + D::SF;
+  Tc* Pw = GY + D::SG;
   const int nt = blockDim.x;
   const int x0 = by * TX, y0 = bx * TY;
   // high-order fluxes of the tile's faces, copied by asynchronous
@@ -1385,17 +1431,44 @@ __device__ __forceinline__ void tile2_final(const double* __restrict__ stage_in,
 #pragma unroll
     for (int v = 0; v < 5; ++v) cp_async_elem(&GY[(v * TX + r) * (TY + 1) + f], p + v * G.vs);
   }
-  cp_async_wait_all();
+  // FP64 launches of a fixed integrator without the fallback: the
+  // Runge-Kutta operands of the tile's cells travel in a second copy group,
+  // beside the flux tiles; each thread later reads only the cells it copied
+  constexpr bool PRE = sizeof(Tc) == 8 && !FB && RKI >= 0 && RKI != INT_RHS;
+  double* const RA = reinterpret_cast<double*>(smem_raw + D::template rk_offset<Tc>(FB));
+  double* const RB = RA + 5 * TX * TY;
+  const int plane = g.nx * g.ny;
+  if constexpr (PRE) {
+    cp_async_commit();
+    const double *A, *B;
+    rk_sources<RKI, RKS, false>(st, A, B);
+    for (int i = threadIdx.x; i < TX * TY; i += nt) {
+      const int r = i / TY, q = i - r * TY;
+      const int x = x0 + r, y = y0 + q;
+      if (x >= g.nx || y >= g.ny) continue;
+      const int o = x * g.ny + y;
+#pragma unroll
+      for (int v = 0; v < 5; ++v) cp_async_elem(&RA[v * TX * TY + i], A + o + v * plane);
+      if (B) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) cp_async_elem(&RB[v * TX * TY + i], B + o + v * plane);
+      }
+    }
+    cp_async_commit();
+    cp_async_wait_group<1>();  // the flux tiles
+  } else {
+    cp_async_wait_all();
+  }
   // fallback at the faces of troubled cells; with predicted flags, faces next
   // to a predicted cell already hold their fallback flux (k2_fluxes) and only
   // the faces of missed cells are revised here. Revising face by face from the
   // stage input instead of the pointwise tile measured slower: misses touch
   // about one face in seven on KH, too many for scattered loads.
-  if (apost && tile_any<TX, TY>(trouble, pred, g, x0, y0)) {
+  if (FB && apost && tile_any<TX, TY>(trouble, pred, g, x0, y0)) {
     // the faces that take the fallback flux, gathered into two lists so that
     // whole warps solve them: solved in place, a warp holding one such face
     // among 32 would run the whole MUSCL + Riemann solve for it
-    int* nface = reinterpret_cast<int*>(GY + D::SG);
+    int* nface = reinterpret_cast<int*>(Pw + D::SP);
     uint16_t* xlist = reinterpret_cast<uint16_t*>(nface + 4);
     uint16_t* ylist = xlist + D::NXF;
     if (threadIdx.x == 0) nface[0] = nface[1] = 0;
@@ -1449,10 +1522,10 @@ __device__ __forceinline__ void tile2_final(const double* __restrict__ stage_in,
       }
     }
   }
+  if constexpr (PRE) cp_async_wait_all();
   __syncthreads();
   // divergence and the Runge-Kutta combination
   const double dt = (RKI >= 0 ? RKI : st.integrator) == INT_RHS ? 0.0 : dt_step;
-  const int plane = g.nx * g.ny;
   unsigned int bad = 0;
   for (int i = threadIdx.x; i < TX * TY; i += nt) {
     const int r = i / TY, q = i - r * TY;
@@ -1466,7 +1539,9 @@ __device__ __forceinline__ void tile2_final(const double* __restrict__ stage_in,
       dc = dc + (Tc)cy * (GY[(v * TX + r) * (TY + 1) + q + 1] - GY[(v * TX + r) * (TY + 1) + q]);
       k[v] = (double)dc;
     }
-    if constexpr (RKI >= 0) {
+    if constexpr (PRE) {
+      bad += rk_combine<RKI, RKS, false>(st, x * g.ny + y, plane, dt, k, RA + i, RB + i, TX * TY);
+    } else if constexpr (RKI >= 0) {
       bad += rk_combine<RKI, RKS, sizeof(Tc) == 4>(st, x * g.ny + y, plane, dt, k);
     } else {
       bad += rk_combine_rt<sizeof(Tc) == 4>(st, x * g.ny + y, plane, dt, k);
@@ -1475,15 +1550,129 @@ __device__ __forceinline__ void tile2_final(const double* __restrict__ stage_in,
   block_count_add(bad, &sc->nonfinite);
 }
 
-// RKI / RKS: the integrator and stage of the launch (one instantiation each)
-template <typename Tc, int TX, int TY, int RKI, int RKS>
-__global__ void __launch_bounds__(256, sizeof(Tc) == 4 ? 5 : 3)
+// Fallback faces of a stage, as one list over the grid: every face with a
+// troubled cell on either side (with predicted flags, only faces with no
+// predicted neighbour: those already hold their fallback flux), as face ids
+// (X faces x*ny + y, then Y faces (nx+1)*ny + x*(ny+1) + y). A block takes
+// FACE_ROUNDS rounds of 256 consecutive faces, counts them per warp and round,
+// reserves its whole segment with one atomic and writes it in face order, so
+// neighbouring list entries are neighbouring faces. Segments land in any
+// order; the revised fluxes do not depend on it (every face is solved on its
+// own). The count is fb_faces (zeroed by k_reset_scalars). One instantiation
+// per compute type (the units of the two precisions each hold one).
+constexpr int FACE_ROUNDS = 8;
+
+__device__ __forceinline__ bool fallback_face(const Geo& g, const uint8_t* __restrict__ trouble,
+                                              const uint8_t* __restrict__ pred, int nxf, int total, int id) {
+  if (id < nxf) {
+    const int x = id / g.ny, y = id - x * g.ny;
+    const int ol = (x - 1) * g.ny + y, orr = x * g.ny + y;
+    const bool need = (x >= 1 && trouble[ol]) || (x < g.nx && trouble[orr]);
+    return need && !(pred && ((x >= 1 && pred[ol]) || (x < g.nx && pred[orr])));
+  }
+  if (id < total) {
+    const int j = id - nxf;
+    const int x = j / (g.ny + 1), y = j - x * (g.ny + 1);
+    const int ol = x * g.ny + y - 1, orr = x * g.ny + y;
+    const bool need = (y >= 1 && trouble[ol]) || (y < g.ny && trouble[orr]);
+    return need && !(pred && ((y >= 1 && pred[ol]) || (y < g.ny && pred[orr])));
+  }
+  return false;
+}
+
+template <typename Tc>
+__global__ void __launch_bounds__(256) k2_face_list(Geo g, const uint8_t* __restrict__ trouble,
+                                                    const uint8_t* __restrict__ pred, int* __restrict__ list,
+                                                    Scalars* __restrict__ sc) {
+  __shared__ int start[FACE_ROUNDS][8];  // per round and warp: its first list slot (then the block's base)
+  __shared__ int block_base;
+  const int nxf = (g.nx + 1) * g.ny, total = nxf + g.nx * (g.ny + 1);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int first = blockIdx.x * (256 * FACE_ROUNDS);
+  unsigned ballot[FACE_ROUNDS];
+#pragma unroll
+  for (int j = 0; j < FACE_ROUNDS; ++j) {
+    ballot[j] = __ballot_sync(0xffffffffu, fallback_face(g, trouble, pred, nxf, total, first + j * 256 + threadIdx.x));
+    if (lane == 0) start[j][warp] = __popc(ballot[j]);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int j = 0; j < FACE_ROUNDS; ++j)
+      for (int w = 0; w < 8; ++w) {
+        const int c = start[j][w];
+        start[j][w] = run;
+        run += c;
+      }
+    block_base = run ? (int)atomicAdd(&sc->fb_faces, (unsigned int)run) : 0;
+  }
+  __syncthreads();
+  const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+  for (int j = 0; j < FACE_ROUNDS; ++j)
+    if ((ballot[j] >> lane) & 1u)
+      list[block_base + start[j][warp] + __popc(ballot[j] & below)] = first + j * 256 + threadIdx.x;
+}
+
+// Fallback fluxes of the listed faces (fvhoe/solver.py:710-732), written over
+// the high-order fluxes in F and G as (1-1)F + 1*F_low: per face, the
+// pointwise primitives of the four cells i-2 .. i+1 along its axis (p = 1
+// reconstruction is the identity), read from the stage input through the
+// ghost maps, then MUSCL and the Riemann solve. Every thread holds a face, so
+// the solves run at the occupancy of the launch instead of waiting on
+// per-tile lists; each face appears once in the list, so no two threads write
+// the same element.
+template <typename Tc>
+__global__ void __launch_bounds__(256) k2_face_solve(const double* __restrict__ stage_in, Geo g, V2<Tc> F, V2<Tc> G,
+                                                     const int* __restrict__ list, int muscl, int limiter,
+                                                     Phys<Tc> ph, Scalars* __restrict__ sc) {
+  const int n = (int)sc->fb_faces;
+  const int nxf = (g.nx + 1) * g.ny;
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&sc->revised_faces, (unsigned int)n);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int id = list[k];
+    const bool xface = id < nxf;
+    int x, y;
+    if (xface) {
+      x = id / g.ny;
+      y = id - x * g.ny;
+    } else {
+      const int j = id - nxf;
+      x = j / (g.ny + 1);
+      y = j - x * (g.ny + 1);
+    }
+    Tc cw[5][4];  // variable v of cell i-2+e at cw[v][e]
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      Tc uc[5], w[5];
+      load_state2<Tc>(stage_in, g, xface ? x - 2 + e : x, xface ? y : y - 2 + e, uc);
+      to_primitives(ph, 5, uc, w);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) cw[v][e] = w[v];
+    }
+    Tc flo[5];
+    fallback_face_flux<Tc>(&cw[0][0], 4, 1, muscl, limiter, ph, xface ? g.dx : g.dy, flo);
+    Tc* o = xface ? F.p + F.at(x, y) : G.p + G.at(x, y);
+    const int vs = xface ? F.vs : G.vs;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      Tc& fh = o[v * vs];
+      fh = (Tc(1) - Tc(1)) * fh + Tc(1) * flo[v];
+    }
+  }
+}
+
+// RKI / RKS: the integrator and stage of the launch (one instantiation each).
+// FB: the fallback fluxes are solved in this launch; without it they are
+// already in F and G (k2_face_list + k2_face_solve).
+template <typename Tc, int TX, int TY, int RKI, int RKS, bool FB>
+__global__ void __launch_bounds__(256, sizeof(Tc) == 4 ? 5 : (FB ? 3 : 4))
     k2_final(const double* __restrict__ stage_in, Geo g, V2<const Tc> F, V2<const Tc> G,
              const uint8_t* __restrict__ trouble, const uint8_t* __restrict__ pred, int apost, int muscl, int limiter,
              Phys<Tc> ph, double cx, double cy, StageSpec st, Scalars* __restrict__ sc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  tile2_final<Tc, TX, TY, RKI, RKS>(stage_in, g, F, G, trouble, pred, apost, muscl, limiter, ph, cx, cy, st,
-                                    RKI == INT_RHS ? 0.0 : sc->dt_step, sc, blockIdx.x, blockIdx.y, smem_raw);
+  tile2_final<Tc, TX, TY, RKI, RKS, FB>(stage_in, g, F, G, trouble, pred, apost, muscl, limiter, ph, cx, cy, st,
+                                        RKI == INT_RHS ? 0.0 : sc->dt_step, sc, blockIdx.x, blockIdx.y, smem_raw);
 }
 
 template <typename Tc, int TX, int TY>
@@ -1491,21 +1680,22 @@ using FinalKernel = void (*)(const double*, Geo, V2<const Tc>, V2<const Tc>, con
                              int, int, Phys<Tc>, double, double, StageSpec, Scalars*);
 
 // The k2_final instantiation of an integrator and stage.
-template <typename Tc, int TX, int TY>
+template <typename Tc, int TX, int TY, bool FB>
 FinalKernel<Tc, TX, TY> final_kernel(int integrator, int stage) {
   switch (integrator) {
-    case INT_EULER: return k2_final<Tc, TX, TY, INT_EULER, 0>;
-    case INT_SSPRK2: return stage == 0 ? k2_final<Tc, TX, TY, INT_SSPRK2, 0> : k2_final<Tc, TX, TY, INT_SSPRK2, 1>;
+    case INT_EULER: return k2_final<Tc, TX, TY, INT_EULER, 0, FB>;
+    case INT_SSPRK2:
+      return stage == 0 ? k2_final<Tc, TX, TY, INT_SSPRK2, 0, FB> : k2_final<Tc, TX, TY, INT_SSPRK2, 1, FB>;
     case INT_SSPRK3:
-      if (stage == 0) return k2_final<Tc, TX, TY, INT_SSPRK3, 0>;
-      if (stage == 1) return k2_final<Tc, TX, TY, INT_SSPRK3, 1>;
-      return k2_final<Tc, TX, TY, INT_SSPRK3, 2>;
+      if (stage == 0) return k2_final<Tc, TX, TY, INT_SSPRK3, 0, FB>;
+      if (stage == 1) return k2_final<Tc, TX, TY, INT_SSPRK3, 1, FB>;
+      return k2_final<Tc, TX, TY, INT_SSPRK3, 2, FB>;
     case INT_RK4:
-      if (stage == 0) return k2_final<Tc, TX, TY, INT_RK4, 0>;
-      if (stage == 1) return k2_final<Tc, TX, TY, INT_RK4, 1>;
-      if (stage == 2) return k2_final<Tc, TX, TY, INT_RK4, 2>;
-      return k2_final<Tc, TX, TY, INT_RK4, 3>;
-    default: return k2_final<Tc, TX, TY, INT_RHS, 0>;
+      if (stage == 0) return k2_final<Tc, TX, TY, INT_RK4, 0, FB>;
+      if (stage == 1) return k2_final<Tc, TX, TY, INT_RK4, 1, FB>;
+      if (stage == 2) return k2_final<Tc, TX, TY, INT_RK4, 2, FB>;
+      return k2_final<Tc, TX, TY, INT_RK4, 3, FB>;
+    default: return k2_final<Tc, TX, TY, INT_RHS, 0, FB>;
   }
 }
 

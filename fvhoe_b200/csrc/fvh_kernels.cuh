@@ -309,6 +309,7 @@ struct Scalars {
   // by the flux pass (faces of predicted cells)
   unsigned int revised_faces;
   unsigned int flux_fallback_faces;
+  unsigned int fb_faces;  // length of this stage's fallback face list (fused 2D path)
 };
 
 // Reduction request for the last transverse sweep of the primitive pass.

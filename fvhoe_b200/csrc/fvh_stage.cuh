@@ -898,11 +898,35 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     if ((st = set_cuda_error(h, "fused detect"))) return st;
   }
   if (pred && (st = mlp_count_stage(h, s))) return st;
-  // 4. fallback + divergence + Runge-Kutta
+  // 4. FP64: fallback fluxes of the troubled faces, written over F and G by
+  // their own launches: the list of those faces (in the sweep scratch, unused
+  // by this path) and its solves. FP32 solves them inside the final pass,
+  // from a pointwise tile per troubled tile (measured faster there; the FP64
+  // final pass holds 3 blocks per SM with the fallback and waits on it).
+  constexpr bool split = sizeof(Tc) == 8;
+  if (apost && split) {
+    const int64_t faces = (int64_t)(g.nx + 1) * g.ny + (int64_t)g.nx * (g.ny + 1);
+    if ((size_t)faces * sizeof(int) > h->buf_elems * sizeof(double)) return fail_config(h, "face list exceeds scratch");
+    {
+      LaunchScope scope(KK_FALLBACK, cells * 1.0, s);  // the flags
+      const unsigned blocks = (unsigned)((faces + 256 * f2::FACE_ROUNDS - 1) / (256 * f2::FACE_ROUNDS));
+      f2::k2_face_list<Tc><<<blocks, 256, 0, s>>>(g, h->trouble, pred, (int*)h->bufA, h->sc);
+      if ((st = set_cuda_error(h, "fused fallback list"))) return st;
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->cfg.device);
+    // the listed faces' states and fluxes: a fraction of the grid, counted as none
+    LaunchScope scope(KK_FALLBACK, 0.0, s);
+    f2::k2_face_solve<Tc><<<(unsigned)(sms * 8), 256, 0, s>>>(c.stage_in, g, F, G, (const int*)h->bufA, 1,
+                                                                 cfg.slope_limiter, ph, h->sc);
+    if ((st = set_cuda_error(h, "fused fallback solve"))) return st;
+  }
+  // 5. (FP32: fallback +) divergence + Runge-Kutta
   {
     using D = f2::FinalDims<T::EX, T::EY>;
-    const size_t smem = (size_t)(D::SP + D::SF + D::SG) * sizeof(Tc) + D::LIST;
-    auto kern = f2::final_kernel<Tc, T::EX, T::EY>(c.spec.integrator, c.spec.stage);
+    // FP64 launches of a stepper stage also stage the Runge-Kutta operands
+    const size_t smem = D::template bytes<Tc>(split && c.spec.integrator != INT_RHS, !split);
+    auto kern = f2::final_kernel<Tc, T::EX, T::EY, !split>(c.spec.integrator, c.spec.stage);
     set_smem((const void*)kern, smem);
     const dim3 grid((g.ny + T::EY - 1) / T::EY, (g.nx + T::EX - 1) / T::EX);
     int arrays = 1;
@@ -914,7 +938,7 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
       case INT_RK4: arrays = c.spec.stage == 0 ? 3 : (c.spec.stage == 3 ? 3 : 4); break;
       default: arrays = 1; break;
     }
-    LaunchScope scope(KK_FINAL, cells * (5 * 2.0 * sizeof(Tc) + arrays * 40.0 + (apost ? 41.0 : 0.0)), s);
+    LaunchScope scope(KK_FINAL, cells * (5 * 2.0 * sizeof(Tc) + arrays * 40.0 + (apost && !split ? 41.0 : 0.0)), s);
     kern<<<grid, 256, smem, s>>>(c.stage_in, g, F.c(), G.c(), h->trouble, pred, apost ? 1 : 0, 1, cfg.slope_limiter, ph,
                                  cx, cy, c.spec, h->sc);
   }

@@ -11,6 +11,7 @@ __global__ void k_reset_scalars(Scalars* sc, int reset_step) {
   if (t == 0) {
     sc->cfl_key = 0ull;
     sc->troubled = 0u;
+    sc->fb_faces = 0u;
     if (reset_step) {
       sc->nonfinite = 0u;
       sc->timeouts = 0u;
