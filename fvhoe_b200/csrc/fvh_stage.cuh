@@ -909,8 +909,9 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
     if ((size_t)faces * sizeof(int) > h->buf_elems * sizeof(double)) return fail_config(h, "face list exceeds scratch");
     {
       LaunchScope scope(KK_FALLBACK, cells * 1.0, s);  // the flags
-      const unsigned blocks = (unsigned)((faces + 256 * f2::FACE_ROUNDS - 1) / (256 * f2::FACE_ROUNDS));
-      f2::k2_face_list<Tc><<<blocks, 256, 0, s>>>(g, h->trouble, pred, (int*)h->bufA, h->sc);
+      // 32 x 32 tiles of the (nx+1) x ny X faces and the nx x (ny+1) Y faces
+      const dim3 tiles((unsigned)(g.ny + 1 + 31) / 32, (unsigned)(g.nx + 1 + 31) / 32);
+      f2::k2_face_list<Tc><<<tiles, 256, 0, s>>>(g, h->trouble, pred, (int*)h->bufA, h->sc);
       if ((st = set_cuda_error(h, "fused fallback list"))) return st;
     }
     int sms = 148;
@@ -925,7 +926,7 @@ int run_stage_fused2d(fvh_handle* h, const StageCall& c, cudaStream_t s) {
   {
     using D = f2::FinalDims<T::EX, T::EY>;
     // FP64 launches of a stepper stage also stage the Runge-Kutta operands
-    const size_t smem = D::template bytes<Tc>(split && c.spec.integrator != INT_RHS, !split);
+    const size_t smem = D::template bytes<Tc>(sizeof(Tc) == 8 && split && c.spec.integrator != INT_RHS, !split);
     auto kern = f2::final_kernel<Tc, T::EX, T::EY, !split>(c.spec.integrator, c.spec.stage);
     set_smem((const void*)kern, smem);
     const dim3 grid((g.ny + T::EY - 1) / T::EY, (g.nx + T::EX - 1) / T::EX);
